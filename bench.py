@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 PairHMM engine (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl rodv|reference]
+                    [--workload uneven] [--scale 1.0]
+
+A step is one pass of the PairHMM forward pass over every pair of the
+workload.  The default workload is the uneven batch: 10,000 regions, 20-200
+reads (50-250 bp) x 2-16 haplotypes (100-600 bp), seeded synthetic data with
+those shapes (rodv_b200/workloads.py); about 10M pairs and 5e11 cells.
+
+Reported (see the JSON keys):
+  value      GCUPS with the batch resident in HBM (rodv_device_batch_run),
+             device time from CUDA events on the engine's stream, summed over
+             the K timed steps; the batch (about 1 GB) is larger than L2.
+  e2e        GCUPS through rodv_pairhmm_batch with host buffers: packing,
+             the H2D copy of the step's inputs from pinned memory, compute and
+             the D2H copy of every result are inside the timed region.
+  roofline   the FP32 forward kernels against the FP32 FMA peak measured on
+             this GPU in this run (FMA-chain kernels, rodv_measure_peaks);
+             12 algorithmic flops per cell (4 mul + 2 add for M, 2 mul + 1 add
+             for I and for D).
+  plain_form the plain GPU form (one launch per pair) against the batched
+             engine on the same sample.
+  cpu_baseline  the reference's own schedule_pairhmm (oracle/_ref), threads
+             over all host cores, on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): one process per GPU; every rank computes its own
+workload of the same shape (seed + rank), no collective on the data path;
+the barrier and max-over-ranks timing use torch.distributed.  ``scaling`` is
+weak.  ``--impl reference`` times the reference's CPU path on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("PairHMM GCUPS on 1 B200 (batched vs plain GPU form, % FP32 peak) vs host AVX; "
+          "p99 ms")
+FLOPS_PER_CELL = 12
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{gpu_index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if not self.proc or not os.path.exists(self.path):
+            return None
+        rows = []
+        for ln in open(self.path):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for _, _, fl in rows for k, v in enumerate(fl)
+                          if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows),
+                "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def cpu_model():
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_rate(batch, threads: int):
+    """The reference's schedule_pairhmm over a batch; returns (GCUPS, seconds)."""
+    import oracle
+    t0 = time.perf_counter()
+    oracle.ref_schedule(batch, threads=threads)
+    dt = time.perf_counter() - t0
+    return batch.cells() / dt / 1e9, dt
+
+
+def sample_for_cpu(name: str, seed: int, target_cells: float):
+    """A seeded prefix of the workload holding about target_cells cells."""
+    from rodv_b200 import workloads
+    full_regions = {"uneven": 10_000, "stream": 1_000, "long": 2_000, "underflow": 200_000,
+                    "plain": 1, "tiny": 8}[name]
+    probe = workloads.make_workload(name, seed=seed, scale=min(1.0, 50 / full_regions))
+    per_region = probe.cells() / max(1, probe.num_regions)
+    n = max(1, min(full_regions, int(target_cells / per_region)))
+    return workloads.make_workload(name, seed=seed, scale=n / full_regions)
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the reference's CPU path, rank 0 only."""
+    if rank != 0:
+        return
+    import oracle
+    threads = os.cpu_count() or 1
+    config = {"workload": args.workload, "scale": args.scale, "sample": "bounded prefix",
+              "l2": "n/a (CPU)"}
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libref_pairhmm.so was not built (reference tree absent "
+                          "at build time)"}))
+        return
+    # ~2e10 cells per step keeps K+W steps within a few minutes on ~8-64 cores
+    target = args.ref_cells_per_step
+    batch = sample_for_cpu(args.workload, 7000, target)
+    warm = sample_for_cpu(args.workload, 7001, target / 20)
+    for _ in range(max(1, args.warmup)):
+        reference_rate(warm, threads)
+    times = []
+    for _ in range(args.steps):
+        _, dt = reference_rate(batch, threads)
+        times.append(dt)
+    total = sum(times)
+    value = batch.cells() * len(times) / total / 1e9
+    sample = (f"{batch.num_regions} regions, {batch.num_pairs} pairs, {batch.cells():.3e} cells "
+              f"of the {args.workload} workload per step")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "GCUPS",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total / len(times) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": config,
+            "cpu_baseline": {"value": value, "unit": "GCUPS", "cores": threads,
+                             "kind": "reference", "sample": sample, "cpu": cpu_model()},
+            "e2e": {"value": value, "unit": "GCUPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_engine(args, world, rank, local):
+    import torch
+    from rodv_b200 import Engine, workloads
+    from rodv_b200.batch import Batch  # noqa: F401
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    t_gen = time.perf_counter()
+    batch = workloads.make_workload(args.workload, seed=workloads.SEEDS[args.workload] + rank,
+                                    scale=args.scale)
+    cells = batch.cells()
+    if rank == 0:
+        log(f"workload {args.workload}: {batch.num_regions} regions, {batch.num_pairs} pairs, "
+            f"{cells:.3e} cells (generated in {time.perf_counter() - t_gen:.1f} s)")
+    eng = Engine(local)
+    peaks = eng.measure_peaks()
+    db = eng.upload(batch)
+
+    # ---- value: device-resident batch ----
+    for _ in range(args.warmup):
+        db.run()
+    barrier()
+    dev_ms, fp32_ms, step_ms, launches, fp64_pairs = [], [], [], 0, 0
+    with Clocks(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ts = time.perf_counter()
+            st = db.run()
+            step_ms.append((time.perf_counter() - ts) * 1e3)
+            dev_ms.append(st["device_ms"])
+            fp32_ms.append(st["fp32_ms"])
+            launches += st["kernel_launches"]
+            fp64_pairs = st["fp64_pairs"]
+        barrier()
+        wall = time.perf_counter() - t0
+    clocks = clk.summary()
+    dev_total = max_over_ranks(sum(dev_ms) / 1e3)
+    value = world * cells * args.steps / dev_total / 1e9
+    results = db.download()
+    db.free()
+
+    # ---- e2e: host buffers through rodv_pairhmm_batch ----
+    from rodv_b200 import _CBatchHolder
+    holder = _CBatchHolder(batch)
+    out = np.empty(batch.num_pairs, dtype=np.float64)
+    for _ in range(max(1, args.warmup // 2)):
+        eng.batch_into(holder, out)
+    barrier()
+    e2e_ms, h2d, d2h = [], 0, 0
+    for _ in range(args.e2e_steps):
+        t = time.perf_counter()
+        st = eng.batch_into(holder, out)
+        e2e_ms.append((time.perf_counter() - t) * 1e3)
+        h2d, d2h = st["h2d_bytes"], st["d2h_bytes"]
+    e2e_total = max_over_ranks(sum(e2e_ms) / 1e3)
+    e2e_value = world * cells * len(e2e_ms) / e2e_total / 1e9
+    same = float(np.abs(out - results).max())
+
+    line = None
+    if rank == 0:
+        fp32_avg_s = sum(fp32_ms) / len(fp32_ms) / 1e3
+        achieved = FLOPS_PER_CELL * cells / fp32_avg_s / 1e12
+        peak = peaks["fp32_gflops"] / 1e3
+        plain = plain_form(eng, args) if args.plain_pairs > 0 else None
+        cpu = None
+        if not args.no_cpu_baseline:
+            cpu = cpu_baseline(args)
+        line = {
+            "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dev_total / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f32x2) + f64 rescue",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "regions": batch.num_regions,
+                       "pairs": batch.num_pairs, "cells": cells, "scale": args.scale,
+                       "l2": "inputs larger than L2 (resident batch ~%.2f GB)" %
+                             (batch.input_bytes() / 1e9),
+                       "parallelism": f"dp{world} (regions sharded, no collective)"},
+            "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "steps": len(e2e_ms),
+                    "ms_per_step": e2e_total / len(e2e_ms) * 1e3,
+                    "max_abs_diff_vs_resident_run": same},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "kernel": "forward_kernel<F32x2,...> (all FP32 classes of a step)",
+                         "flops_per_cell": FLOPS_PER_CELL,
+                         "peak_source": "FFMA-chain kernel measured in this run "
+                                        "(rodv_measure_peaks); MEASURED_PEAKS.json has no "
+                                        "FP32 entry",
+                         "fp32x2_peak_tflops": peaks["fp32x2_gflops"] / 1e3,
+                         "fp64_peak_tflops": peaks["fp64_gflops"] / 1e3,
+                         "peak_sm_mhz": peaks["sm_mhz"]},
+            "fp64_rescue": {"pairs": int(fp64_pairs),
+                            "rate": fp64_pairs / max(1, batch.num_pairs)},
+            "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
+                           "p99": float(np.percentile(step_ms, 99)),
+                           "what": "per-step (whole batch) host-observed latency"},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "wall_s_timed": wall,
+        }
+        if plain:
+            line["plain_form"] = plain
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    eng.close()
+
+
+def plain_form(eng, args):
+    """Plain one-pair-per-launch GPU form vs the batched engine on one sample."""
+    from rodv_b200 import workloads
+    b = workloads.make_workload("plain")  # 1 region, 8 x 64 pairs
+    db = eng.upload(b)
+    db.run()
+    reps = 5
+    t_batched = []
+    for _ in range(reps):
+        t_batched.append(db.run()["device_ms"])
+    _, st = eng.plain(db)
+    db.free()
+    cells = b.cells()
+    batched = cells / (min(t_batched) / 1e3) / 1e9
+    plain = cells / (st["device_ms"] / 1e3) / 1e9
+    return {"sample": f"plain workload: 1 region, {b.num_pairs} pairs, {cells:.3e} cells",
+            "plain_gcups": plain, "batched_gcups": batched, "speedup": batched / plain,
+            "plain_launches": st["kernel_launches"]}
+
+
+def cpu_baseline(args):
+    import oracle
+    if not oracle.ref_available():
+        return {"value": None, "unit": "GCUPS", "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref was not built"}
+    threads = os.cpu_count() or 1
+    batch = sample_for_cpu(args.workload, 7000, args.ref_cells_per_step)
+    warm = sample_for_cpu(args.workload, 7001, args.ref_cells_per_step / 20)
+    reference_rate(warm, threads)
+    rate, dt = reference_rate(batch, threads)
+    return {"value": rate, "unit": "GCUPS", "cores": threads, "kind": "reference",
+            "sample": f"{batch.num_regions} regions / {batch.num_pairs} pairs / "
+                      f"{batch.cells():.3e} cells of the {args.workload} workload, "
+                      f"{dt:.1f} s on {threads} threads",
+            "cpu": cpu_model()}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["rodv", "reference"], default="rodv")
+    ap.add_argument("--workload", default="uneven")
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--plain-pairs", type=int, default=512)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-cells-per-step", type=float, default=2e10)
+    args = ap.parse_args()
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_engine(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,174 @@
+/*
+ * rodv_pairhmm.h -- C ABI of the B200 PairHMM engine.
+ *
+ * The engine computes, for every (haplotype, read) pair of every region in a
+ * batch, the PairHMM forward log10 likelihood that roDV's src/core batch API
+ * computes on the CPU.  All functions are plain C: caller-owned host
+ * buffers, engine-owned device state, integer status codes, no exceptions
+ * across the boundary.  One engine may be shared by several host threads;
+ * calls on one engine are serialised internally.
+ *
+ * Reference interfaces replaced (paths relative to the roDV repository):
+ *   pairhmm::schedule::schedule_pairhmm     src/core/pairhmm_schedule.h:14-25
+ *       -> rodv_pairhmm_batch (and the C++ shim of the same name in
+ *          rodv_b200/csrc/schedule_shim.cpp, declared in
+ *          include/rodv_pairhmm_schedule.h)
+ *   pairhmm::intra::computeLikelihoodsAVX2/AVX512
+ *                                           src/core/pairhmm/intra/pairhmm_api.h:17-20
+ *       -> rodv_pairhmm_pair
+ *   pairhmm::inter::compute_inter_pairhmm_{AVX2,AVX512}_{float,double}
+ *                                           src/core/pairhmm/inter/pairhmm_inter_api.h:17-24
+ *       -> rodv_pairhmm_batch with one single-pair region per test case
+ */
+#ifndef RODV_PAIRHMM_H_
+#define RODV_PAIRHMM_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RODV_ABI_VERSION 1
+
+typedef int32_t rodv_status;
+enum {
+  RODV_OK = 0,
+  RODV_ERR_INVALID_ARG = 1,   /* null pointer, bad index, zero length, quals length mismatch */
+  RODV_ERR_EMPTY = 2,         /* a region with no haplotypes or no reads (reference returns
+                                 false, pairhmm_schedule.cpp:130-132) */
+  RODV_ERR_INVALID_BASE = 3,  /* a base other than A, C, G, T, N */
+  RODV_ERR_NO_DEVICE = 4,     /* no CUDA device, or the library was built for another arch */
+  RODV_ERR_CUDA = 5,          /* a CUDA runtime call failed */
+  RODV_ERR_OUT_OF_MEMORY = 6, /* device or pinned host allocation failed */
+  RODV_ERR_TOO_LONG = 7,      /* read or haplotype above the engine limits */
+  RODV_ERR_DEVICE_CHECK = 8,  /* a kernel reported a bad descriptor or an expired wait */
+  RODV_ERR_ADMISSION = 9,     /* streaming: region does not fit the device memory budget */
+  RODV_ERR_NOT_FOUND = 10,    /* streaming: unknown ticket */
+  RODV_ERR_NOT_READY = 11,    /* streaming: result not yet available */
+  RODV_ERR_SHUTDOWN = 12      /* streaming: service stopped */
+};
+
+/* Engine limits (inputs beyond them are rejected with RODV_ERR_TOO_LONG). */
+#define RODV_MAX_READ_LEN 65536u
+#define RODV_MAX_HAP_LEN 65536u
+
+/* A region is roDV's schedule_pairhmm call: haplotypes [hap_start,
+ * hap_start+num_haps) against reads [read_start, read_start+num_reads). */
+typedef struct rodv_region {
+  uint32_t hap_start;
+  uint32_t num_haps;
+  uint32_t read_start;
+  uint32_t num_reads;
+} rodv_region;
+
+/* A batch of regions over flat host arrays.  Bases are ASCII A/C/G/T/N;
+ * qualities are raw Phred integers (not +33), one per read base in each of
+ * the four arrays (base, insertion, deletion, gap continuation), masked with
+ * &127 as the reference does.  Results of region g are written hap-major
+ * (result[h][r] of schedule_pairhmm) starting at sum over g' < g of
+ * num_haps*num_reads. */
+typedef struct rodv_batch {
+  uint32_t num_regions;
+  const rodv_region* regions;
+  uint32_t num_haps;
+  const uint8_t* hap_bases;
+  const uint64_t* hap_offsets;
+  const uint32_t* hap_lengths;
+  uint32_t num_reads;
+  const uint8_t* read_bases;
+  const uint8_t* base_quals;
+  const uint8_t* ins_quals;
+  const uint8_t* del_quals;
+  const uint8_t* gcp_quals;
+  const uint64_t* read_offsets; /* shared by read_bases and the four quality arrays */
+  const uint32_t* read_lengths;
+} rodv_batch;
+
+typedef struct rodv_options {
+  int32_t device;               /* CUDA device ordinal */
+  int32_t force_fp64;           /* 1: every pair in FP64 (schedule_pairhmm use_double) */
+  uint64_t device_memory_budget;/* bytes the streaming service may hold; 0 = 50% of free */
+  uint32_t max_inflight;        /* streaming: regions admitted at once; 0 = 4096 */
+  int32_t verbose;              /* 1: print per-batch statistics to stderr */
+} rodv_options;
+
+typedef struct rodv_stats {
+  uint64_t pairs;               /* pairs computed */
+  uint64_t cells;               /* sum of read_len * hap_len over pairs */
+  uint64_t fp64_pairs;          /* pairs computed in FP64 (rescued or forced) */
+  uint64_t fp64_cells;
+  uint32_t kernel_launches;     /* forward/pack kernels launched by this call */
+  uint32_t pad_;
+  double total_ms;              /* wall time of the call */
+  double device_ms;             /* device time of the forward kernels (CUDA events) */
+  double fp32_ms;               /* device time of the FP32 pass */
+  double h2d_ms;
+  double d2h_ms;
+  uint64_t h2d_bytes;
+  uint64_t d2h_bytes;
+} rodv_stats;
+
+typedef struct rodv_engine rodv_engine;
+typedef struct rodv_device_batch rodv_device_batch;
+
+/* Fills opts with defaults (device 0, FP32 with FP64 rescue). */
+void rodv_default_options(rodv_options* opts);
+
+rodv_status rodv_engine_create(const rodv_options* opts, rodv_engine** out);
+void rodv_engine_destroy(rodv_engine* engine);
+
+/* Whole batch, host buffers in and out: pack, upload, compute, download.
+ * Replaces schedule_pairhmm (pairhmm_schedule.h:14-25) for many regions at
+ * once; out_log10 holds rodv_batch_num_pairs(batch) doubles.  use_double != 0
+ * computes every pair in FP64 (schedule_pairhmm's use_double); otherwise
+ * FP32 with FP64 rescue below 1e-28.  stats may be null. */
+rodv_status rodv_pairhmm_batch(rodv_engine* engine, const rodv_batch* batch, int32_t use_double,
+                               double* out_log10, rodv_stats* stats);
+
+/* Number of results of a batch (sum of num_haps*num_reads). */
+uint64_t rodv_batch_num_pairs(const rodv_batch* batch);
+
+/* One pair (computeLikelihoodsAVX512(tc, use_double), pairhmm_api.h:17-20):
+ * FP32 with FP64 rescue below 1e-28, or FP64 when use_double != 0. */
+rodv_status rodv_pairhmm_pair(rodv_engine* engine, const uint8_t* hap, uint32_t hap_len,
+                              const uint8_t* read, const uint8_t* base_quals,
+                              const uint8_t* ins_quals, const uint8_t* del_quals,
+                              const uint8_t* gcp_quals, uint32_t read_len, int32_t use_double,
+                              double* out_log10);
+
+/* Device-resident batches: upload once, run many times, read results.
+ * rodv_device_batch_run computes with inputs already in HBM (no host
+ * copies); results stay on the device until rodv_device_batch_download. */
+rodv_status rodv_device_batch_upload(rodv_engine* engine, const rodv_batch* batch,
+                                     rodv_device_batch** out);
+rodv_status rodv_device_batch_run(rodv_engine* engine, rodv_device_batch* dbatch,
+                                  rodv_stats* stats);
+rodv_status rodv_device_batch_download(rodv_engine* engine, rodv_device_batch* dbatch,
+                                       double* out_log10);
+void rodv_device_batch_free(rodv_engine* engine, rodv_device_batch* dbatch);
+
+/* The plain GPU form: one kernel launch per pair (plus one FP64 launch for a
+ * pair below the threshold) over a device-resident batch, results downloaded
+ * to out_log10.  Kept as the comparison point for the batched engine. */
+rodv_status rodv_pairhmm_plain(rodv_engine* engine, rodv_device_batch* dbatch,
+                               double* out_log10, rodv_stats* stats);
+
+/* Arithmetic peak of the device, measured by FMA-chain kernels: FP32 FFMA,
+ * FP32x2 FFMA2 and FP64 DFMA, in GFLOP/s, and the SM clock in MHz seen
+ * during the FP32 run (from clock64 against CUDA events). */
+rodv_status rodv_measure_peaks(rodv_engine* engine, double* fp32_gflops, double* fp32x2_gflops,
+                               double* fp64_gflops, double* sm_mhz);
+
+/* Human-readable name of a status code (static storage). */
+const char* rodv_status_string(rodv_status status);
+
+/* Details of the last failure on this engine (static until the next call). */
+const char* rodv_last_error(rodv_engine* engine);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RODV_PAIRHMM_H_ */

@@ -1,0 +1,164 @@
+// capi.cpp -- extern "C" entry points of include/rodv_pairhmm.h.
+#include <cstring>
+#include <mutex>
+#include <new>
+
+#include "engine.h"
+
+using rodv::Engine;
+
+extern "C" {
+
+void rodv_default_options(rodv_options* opts) {
+  if (!opts) return;
+  std::memset(opts, 0, sizeof(*opts));
+  opts->device = 0;
+  opts->force_fp64 = 0;
+  opts->device_memory_budget = 0;
+  opts->max_inflight = 0;
+  opts->verbose = 0;
+}
+
+rodv_status rodv_engine_create(const rodv_options* opts, rodv_engine** out) {
+  if (!out) return RODV_ERR_INVALID_ARG;
+  *out = nullptr;
+  rodv_options o;
+  rodv_default_options(&o);
+  if (opts) o = *opts;
+  Engine* e = new (std::nothrow) Engine(o);
+  if (!e) return RODV_ERR_OUT_OF_MEMORY;
+  rodv_status s = e->init();
+  if (s != RODV_OK) {
+    delete e;
+    return s;
+  }
+  *out = new (std::nothrow) rodv_engine{e};
+  if (!*out) {
+    delete e;
+    return RODV_ERR_OUT_OF_MEMORY;
+  }
+  return RODV_OK;
+}
+
+void rodv_engine_destroy(rodv_engine* engine) {
+  if (!engine) return;
+  delete engine->impl;
+  delete engine;
+}
+
+uint64_t rodv_batch_num_pairs(const rodv_batch* b) {
+  if (!b || !b->regions) return 0;
+  uint64_t n = 0;
+  for (uint32_t g = 0; g < b->num_regions; ++g)
+    n += (uint64_t)b->regions[g].num_haps * b->regions[g].num_reads;
+  return n;
+}
+
+rodv_status rodv_pairhmm_batch(rodv_engine* engine, const rodv_batch* batch, int32_t use_double,
+                               double* out, rodv_stats* stats) {
+  if (!engine || !batch) return RODV_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(engine->impl->mutex());
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  return engine->impl->run_host(*batch, out, stats, use_double != 0);
+}
+
+rodv_status rodv_pairhmm_pair(rodv_engine* engine, const uint8_t* hap, uint32_t hap_len,
+                              const uint8_t* read, const uint8_t* q, const uint8_t* ins,
+                              const uint8_t* del, const uint8_t* gcp, uint32_t read_len,
+                              int32_t use_double, double* out) {
+  if (!engine || !hap || !read || !q || !ins || !del || !gcp || !out)
+    return RODV_ERR_INVALID_ARG;
+  if (read_len == 0 || hap_len == 0) return RODV_ERR_INVALID_ARG;
+  // One region, one haplotype, one read; the read's four quality arrays
+  // are separate buffers, so the batch's shared read_offsets is 0 for each.
+  rodv_region rg{0, 1, 0, 1};
+  const uint64_t zero = 0;
+  rodv_batch b{};
+  b.num_regions = 1;
+  b.regions = &rg;
+  b.num_haps = 1;
+  b.hap_bases = hap;
+  b.hap_offsets = &zero;
+  b.hap_lengths = &hap_len;
+  b.num_reads = 1;
+  b.read_bases = read;
+  b.base_quals = q;
+  b.ins_quals = ins;
+  b.del_quals = del;
+  b.gcp_quals = gcp;
+  b.read_offsets = &zero;
+  b.read_lengths = &read_len;
+  std::lock_guard<std::mutex> lk(engine->impl->mutex());
+  return engine->impl->run_host(b, out, nullptr, use_double != 0);
+}
+
+rodv_status rodv_device_batch_upload(rodv_engine* engine, const rodv_batch* batch,
+                                     rodv_device_batch** out) {
+  if (!engine || !batch || !out) return RODV_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(engine->impl->mutex());
+  return engine->impl->upload(*batch, out);
+}
+
+rodv_status rodv_device_batch_run(rodv_engine* engine, rodv_device_batch* db, rodv_stats* stats) {
+  if (!engine || !db) return RODV_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(engine->impl->mutex());
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  return engine->impl->run_device(db, stats);
+}
+
+rodv_status rodv_device_batch_download(rodv_engine* engine, rodv_device_batch* db, double* out) {
+  if (!engine || !db || !out) return RODV_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(engine->impl->mutex());
+  return engine->impl->download(db, out);
+}
+
+void rodv_device_batch_free(rodv_engine* engine, rodv_device_batch* db) {
+  if (!db) return;
+  if (engine) {
+    std::lock_guard<std::mutex> lk(engine->impl->mutex());
+    delete db;
+  } else {
+    delete db;
+  }
+}
+
+rodv_status rodv_pairhmm_plain(rodv_engine* engine, rodv_device_batch* db, double* out,
+                               rodv_stats* stats) {
+  if (!engine || !db) return RODV_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(engine->impl->mutex());
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  return engine->impl->plain(db, out, stats);
+}
+
+rodv_status rodv_measure_peaks(rodv_engine* engine, double* f32, double* f32x2, double* f64,
+                               double* mhz) {
+  if (!engine) return RODV_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(engine->impl->mutex());
+  return engine->impl->measure_peaks(f32, f32x2, f64, mhz);
+}
+
+const char* rodv_status_string(rodv_status s) {
+  switch (s) {
+    case RODV_OK: return "ok";
+    case RODV_ERR_INVALID_ARG: return "invalid argument";
+    case RODV_ERR_EMPTY: return "region without haplotypes or reads";
+    case RODV_ERR_INVALID_BASE: return "base outside A, C, G, T, N";
+    case RODV_ERR_NO_DEVICE: return "no usable CUDA device";
+    case RODV_ERR_CUDA: return "CUDA runtime error";
+    case RODV_ERR_OUT_OF_MEMORY: return "out of memory";
+    case RODV_ERR_TOO_LONG: return "input above engine limits";
+    case RODV_ERR_DEVICE_CHECK: return "device-side check failed";
+    case RODV_ERR_ADMISSION: return "region does not fit the device memory budget";
+    case RODV_ERR_NOT_FOUND: return "unknown ticket";
+    case RODV_ERR_NOT_READY: return "result not ready";
+    case RODV_ERR_SHUTDOWN: return "service stopped";
+    default: return "unknown status";
+  }
+}
+
+const char* rodv_last_error(rodv_engine* engine) {
+  if (!engine) return "";
+  return engine->impl->last_error();
+}
+
+}  // extern "C"

@@ -1,0 +1,741 @@
+// engine.cu -- host side of the PairHMM engine: validation, packing, class
+// planning, persistent launches, FP64 rescue, results.
+//
+// Control flow of one batch (the B200 counterpart of schedule_pairhmm,
+// src/core/pairhmm_schedule.cpp:116-340):
+//   1. validate and pack on the host (threads over reads) into one pinned
+//      staging buffer laid out exactly like the device arena;
+//   2. one H2D copy of the staging buffer;
+//   3. for each work class with pairs, one persistent FP32 launch over its
+//      items (two pairs per warp); pairs whose scaled FP32 result is below
+//      1e-28 are appended to the class's rescue list on the device;
+//   4. for each class, one persistent FP64 launch that drains the rescue list
+//      (its length is read by the kernel, never by the host);
+//   5. one D2H copy of the log10 results.
+// The reference instead groups pairs into SIMD-width groups by padded area
+// (greedy_grouping, :46-105) and sends leftovers to a per-pair kernel; on the
+// GPU every pair goes through the same batched kernels, and work classes
+// (rows per lane) play the part of its idle-ratio grouping.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <thread>
+
+#include "engine.h"
+#include "tables.h"
+
+namespace rodv {
+
+namespace {
+
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t v, size_t a = kAlign) { return (v + a - 1) / a * a; }
+
+// A0 C1 G2 T3 N4; 0xff marks a base outside the engine's domain.
+struct CodeTable {
+  uint8_t v[256];
+  CodeTable() {
+    std::memset(v, 0xff, sizeof(v));
+    v['A'] = kA; v['C'] = kC; v['G'] = kG; v['T'] = kT; v['N'] = kN;
+  }
+};
+const CodeTable kCodes;
+
+template <class F>
+void parallel_for(size_t n, size_t grain, F&& f) {
+  unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t chunks = (n + grain - 1) / grain;
+  const unsigned nt = (unsigned)std::min<size_t>(hw, chunks);
+  if (nt <= 1) {
+    if (n) f(0, n);
+    return;
+  }
+  std::atomic<size_t> next{0};
+  std::vector<std::thread> pool;
+  pool.reserve(nt);
+  for (unsigned t = 0; t < nt; ++t) {
+    pool.emplace_back([&] {
+      for (;;) {
+        const size_t c = next.fetch_add(1);
+        if (c >= chunks) break;
+        f(c * grain, std::min(n, (c + 1) * grain));
+      }
+    });
+  }
+  for (auto& th : pool) th.join();
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Device-arena views of a packed plan.
+struct ArenaView {
+  BatchView view;
+  uint32_t* counts;   // [kNumClasses] fp32 counters, [kNumClasses] fp64 counters,
+                      // [kNumClasses] rescue counts, [1] error flags
+  float* scratch;
+};
+
+ArenaView arena_view(const PackedPlan& p, uint8_t* base, const PriorTables& tab) {
+  ArenaView a;
+  a.view.hap_codes = base + p.off_hap_codes;
+  a.view.read_rows = reinterpret_cast<const uint32_t*>(base + p.off_read_rows);
+  a.view.haps = reinterpret_cast<const HapDesc*>(base + p.off_haps);
+  a.view.reads = reinterpret_cast<const ReadDesc*>(base + p.off_reads);
+  a.view.pairs = reinterpret_cast<const PairDesc*>(base + p.off_pairs);
+  a.view.out = reinterpret_cast<double*>(base + p.off_out);
+  a.view.tab = tab;
+  a.counts = reinterpret_cast<uint32_t*>(base + p.off_counts);
+  a.scratch = p.scratch_bytes ? reinterpret_cast<float*>(base + p.off_scratch) : nullptr;
+  return a;
+}
+constexpr int kCountWords = 3 * kNumClasses + 1;
+
+}  // namespace
+
+DeviceMem::~DeviceMem() {
+  if (ptr) cudaFree(ptr);
+}
+cudaError_t DeviceMem::ensure(size_t n) {
+  if (n <= bytes && ptr) return cudaSuccess;
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+  cudaError_t e = cudaMalloc(&ptr, std::max<size_t>(n, 1));
+  if (e == cudaSuccess) bytes = n;
+  return e;
+}
+PinnedMem::~PinnedMem() {
+  if (ptr) cudaFreeHost(ptr);
+}
+cudaError_t PinnedMem::ensure(size_t n) {
+  if (n <= bytes && ptr) return cudaSuccess;
+  if (ptr) cudaFreeHost(ptr);
+  ptr = nullptr;
+  bytes = 0;
+  cudaError_t e = cudaMallocHost(&ptr, std::max<size_t>(n, 1));
+  if (e == cudaSuccess) bytes = n;
+  return e;
+}
+
+Engine::Engine(const rodv_options& opt) : opt_(opt) {}
+
+Engine::~Engine() {
+  if (ready_) {
+    cudaSetDevice(device_);
+    cudaStreamSynchronize(stream_);
+    for (auto& e : ev_) cudaEventDestroy(e);
+    cudaStreamDestroy(stream_);
+  }
+}
+
+rodv_status Engine::fail(rodv_status s, const std::string& msg) {
+  last_error_ = msg;
+  if (opt_.verbose) fprintf(stderr, "rodv: %s\n", msg.c_str());
+  return s;
+}
+
+rodv_status Engine::cuda_fail(cudaError_t e, const char* where) {
+  const rodv_status s = (e == cudaErrorMemoryAllocation) ? RODV_ERR_OUT_OF_MEMORY : RODV_ERR_CUDA;
+  return fail(s, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define RODV_CUDA(call)                                   \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
+  } while (0)
+
+rodv_status Engine::init() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+    return fail(RODV_ERR_NO_DEVICE, "no CUDA device visible");
+  if (opt_.device < 0 || opt_.device >= n)
+    return fail(RODV_ERR_NO_DEVICE, "device ordinal out of range");
+  device_ = opt_.device;
+  RODV_CUDA(cudaSetDevice(device_));
+  cudaDeviceProp prop;
+  RODV_CUDA(cudaGetDeviceProperties(&prop, device_));
+  if (prop.major != 10 || prop.minor != 0)
+    return fail(RODV_ERR_NO_DEVICE, std::string("engine is built for sm_100a; device is ") +
+                                        prop.name);
+  num_sms_ = prop.multiProcessorCount;
+  RODV_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  for (auto& e : ev_) RODV_CUDA(cudaEventCreate(&e));
+  const HostPriorTables& t = host_prior_tables();
+  const size_t bytes = 128 * 4 + kMmTableSize * 4 + 128 * 8 + kMmTableSize * 8 + 4 * kAlign;
+  RODV_CUDA(tables_.ensure(bytes));
+  uint8_t* base = static_cast<uint8_t*>(tables_.ptr);
+  size_t o = 0;
+  auto put = [&](const void* src, size_t n) -> void* {
+    void* dst = base + o;
+    cudaMemcpy(dst, src, n, cudaMemcpyHostToDevice);
+    o = align_up(o + n);
+    return dst;
+  };
+  tab_.ph2pr_f = static_cast<const float*>(put(t.ph2pr_f.data(), 128 * 4));
+  tab_.mm_f = static_cast<const float*>(put(t.mm_f.data(), kMmTableSize * 4));
+  tab_.ph2pr_d = static_cast<const double*>(put(t.ph2pr_d.data(), 128 * 8));
+  tab_.mm_d = static_cast<const double*>(put(t.mm_d.data(), kMmTableSize * 8));
+  RODV_CUDA(cudaGetLastError());
+  ready_ = true;
+  return RODV_OK;
+}
+
+int Engine::persistent_blocks(const KernelInfo& k) const {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.threads, k.smem_bytes) !=
+          cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  return per_sm * num_sms_;
+}
+
+// ---------------------------------------------------------------------------
+// Packing
+// ---------------------------------------------------------------------------
+rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64) {
+  plan = PackedPlan{};
+  plan.fp64 = fp64;
+  if (b.num_regions == 0 || !b.regions) return fail(RODV_ERR_EMPTY, "batch has no regions");
+  if (!b.hap_bases || !b.hap_offsets || !b.hap_lengths || !b.read_bases || !b.base_quals ||
+      !b.ins_quals || !b.del_quals || !b.gcp_quals || !b.read_offsets || !b.read_lengths)
+    return fail(RODV_ERR_INVALID_ARG, "null array in batch");
+  // regions
+  uint64_t pairs = 0;
+  for (uint32_t g = 0; g < b.num_regions; ++g) {
+    const rodv_region& r = b.regions[g];
+    if (r.num_haps == 0 || r.num_reads == 0)
+      return fail(RODV_ERR_EMPTY, "region " + std::to_string(g) + " has no haplotypes or reads");
+    if ((uint64_t)r.hap_start + r.num_haps > b.num_haps ||
+        (uint64_t)r.read_start + r.num_reads > b.num_reads)
+      return fail(RODV_ERR_INVALID_ARG, "region " + std::to_string(g) + " indexes out of range");
+    pairs += (uint64_t)r.num_haps * r.num_reads;
+  }
+  if (pairs >= 0xffffffffull) return fail(RODV_ERR_TOO_LONG, "batch has 2^32 or more pairs");
+  plan.num_pairs = pairs;
+  plan.num_haps = b.num_haps;
+  plan.num_reads = b.num_reads;
+
+  // haplotype code buffer: [pad][hap 0][pad][hap 1]...[hap n-1][pad + max len]
+  std::vector<uint64_t> hap_code_off(b.num_haps);
+  uint64_t hb = 0;
+  uint32_t max_h = 0;
+  for (uint32_t h = 0; h < b.num_haps; ++h) {
+    const uint32_t len = b.hap_lengths[h];
+    if (len == 0) return fail(RODV_ERR_INVALID_ARG, "haplotype " + std::to_string(h) + " is empty");
+    if (len > RODV_MAX_HAP_LEN) return fail(RODV_ERR_TOO_LONG, "haplotype longer than limit");
+    hb += kHapPad;
+    hap_code_off[h] = hb;
+    hb += len;
+    max_h = std::max(max_h, len);
+  }
+  hb += kHapPad + max_h + kHapPad;
+  plan.hap_code_bytes = hb;
+  plan.max_hap_len = max_h;
+
+  std::vector<uint64_t> row_off(b.num_reads);
+  uint64_t rows = 0;
+  for (uint32_t r = 0; r < b.num_reads; ++r) {
+    const uint32_t len = b.read_lengths[r];
+    if (len == 0) return fail(RODV_ERR_INVALID_ARG, "read " + std::to_string(r) + " is empty");
+    if (len > RODV_MAX_READ_LEN) return fail(RODV_ERR_TOO_LONG, "read longer than limit");
+    row_off[r] = rows;
+    rows += (len + 3) & ~3u;
+  }
+  plan.read_rows = rows;
+
+  // ---- arena layout ----
+  size_t o = 0;
+  plan.off_hap_codes = o; o = align_up(o + hb);
+  plan.off_read_rows = o; o = align_up(o + rows * 4);
+  plan.off_haps = o; o = align_up(o + (size_t)b.num_haps * sizeof(HapDesc));
+  plan.off_reads = o; o = align_up(o + (size_t)b.num_reads * sizeof(ReadDesc));
+  plan.off_pairs = o; o = align_up(o + pairs * sizeof(PairDesc));
+  // class counts need read flags first: compute them with the read pass below
+  // (item/list offsets are filled after counting).
+  const size_t fixed_end = o;
+
+  // ---- pass 1: read flags (uniform gaps) and class of every read ----
+  std::vector<uint8_t> read_uniform(b.num_reads);
+  std::atomic<int> bad_base{-1};
+  parallel_for(b.num_reads, 4096, [&](size_t lo, size_t hi) {
+    for (size_t r = lo; r < hi; ++r) {
+      const uint64_t off = b.read_offsets[r];
+      const uint32_t n = b.read_lengths[r];
+      const uint8_t i0 = b.ins_quals[off] & 127, d0 = b.del_quals[off] & 127,
+                    c0 = b.gcp_quals[off] & 127;
+      bool u = true;
+      for (uint32_t k = 1; k < n && u; ++k)
+        u = (b.ins_quals[off + k] & 127) == i0 && (b.del_quals[off + k] & 127) == d0 &&
+            (b.gcp_quals[off + k] & 127) == c0;
+      // The uniform-gap kernels store M/gapm; gcp quality 0 gives gapm = 0,
+      // so such reads take the per-row kernels.
+      read_uniform[r] = (u && c0 != 0) ? 1 : 0;
+    }
+  });
+  std::vector<uint8_t> read_class(b.num_reads);
+  for (uint32_t r = 0; r < b.num_reads; ++r)
+    read_class[r] = (uint8_t)class_of(b.read_lengths[r], read_uniform[r] != 0);
+
+  // ---- per-class pair counts and the largest haplotype of multi-pass pairs ----
+  for (uint32_t g = 0; g < b.num_regions; ++g) {
+    const rodv_region& rg = b.regions[g];
+    uint32_t rc[kNumClasses] = {};
+    for (uint32_t r = 0; r < rg.num_reads; ++r) rc[read_class[rg.read_start + r]]++;
+    for (int c = 0; c < kNumClasses; ++c) plan.pairs[c] += rc[c] * rg.num_haps;
+    if (rc[kSinglePassClasses] || rc[kSinglePassClasses + 1])
+      for (uint32_t h = 0; h < rg.num_haps; ++h)
+        plan.multi_max_hap = std::max(plan.multi_max_hap, b.hap_lengths[rg.hap_start + h]);
+  }
+  o = fixed_end;
+  for (int c = 0; c < kNumClasses; ++c) {
+    plan.items[c] = fp64 ? 0 : (plan.pairs[c] + 1) / 2;
+    plan.off_items[c] = o;
+    o = align_up(o + (size_t)plan.items[c] * sizeof(Item));
+    plan.off_lists[c] = o;
+    o = align_up(o + (size_t)plan.pairs[c] * 4);
+  }
+  plan.upload_bytes = o;
+  plan.off_out = o; o = align_up(o + pairs * 8);
+  plan.off_counts = o; o = align_up(o + kCountWords * 4);
+  plan.scratch_cols = plan.multi_max_hap ? plan.multi_max_hap + 40 : 0;
+  plan.off_scratch = o;
+  if (plan.scratch_cols) {
+    int blocks = 0, warps = 0;
+    for (int u = 0; u < 2; ++u)
+      for (int p = 0; p < 2; ++p) {
+        const KernelInfo k = forward_kernel_info(p ? Precision::kF64 : Precision::kF32x2,
+                                                 kMaxRowsPerLane, u != 0, true);
+        blocks = persistent_blocks(k);
+        warps = std::max(warps, blocks * k.warps_per_block);
+      }
+    plan.scratch_bytes = (size_t)warps * plan.scratch_cols * 24;
+    o = align_up(o + plan.scratch_bytes);
+  }
+  plan.total_bytes = o;
+
+  cudaError_t e = staging.ensure(plan.upload_bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "pinned staging allocation");
+  uint8_t* s = static_cast<uint8_t*>(staging.ptr);
+
+  // ---- haplotype codes ----
+  uint8_t* codes = s + plan.off_hap_codes;
+  std::memset(codes, 0, hb);
+  HapDesc* hd = reinterpret_cast<HapDesc*>(s + plan.off_haps);
+  parallel_for(b.num_haps, 256, [&](size_t lo, size_t hi) {
+    for (size_t h = lo; h < hi; ++h) {
+      const uint8_t* src = b.hap_bases + b.hap_offsets[h];
+      uint8_t* dst = codes + hap_code_off[h];
+      const uint32_t n = b.hap_lengths[h];
+      for (uint32_t k = 0; k < n; ++k) {
+        const uint8_t c = kCodes.v[src[k]];
+        if (c == 0xff) bad_base.store((int)src[k]);
+        dst[k] = c;
+      }
+      hd[h].code_off = hap_code_off[h];
+      hd[h].len = n;
+      hd[h].pad_ = 0;
+    }
+  });
+  // ---- read rows ----
+  uint32_t* rw = reinterpret_cast<uint32_t*>(s + plan.off_read_rows);
+  ReadDesc* rdesc = reinterpret_cast<ReadDesc*>(s + plan.off_reads);
+  parallel_for(b.num_reads, 1024, [&](size_t lo, size_t hi) {
+    for (size_t r = lo; r < hi; ++r) {
+      const uint64_t off = b.read_offsets[r];
+      const uint32_t n = b.read_lengths[r];
+      uint32_t* dst = rw + row_off[r];
+      for (uint32_t k = 0; k < n; ++k) {
+        const uint8_t c = kCodes.v[b.read_bases[off + k]];
+        if (c == 0xff) bad_base.store((int)b.read_bases[off + k]);
+        dst[k] = row_word(c, b.base_quals[off + k], b.ins_quals[off + k], b.del_quals[off + k],
+                          b.gcp_quals[off + k]);
+      }
+      for (uint32_t k = n; k < ((n + 3) & ~3u); ++k) dst[k] = 0;
+      rdesc[r].row_off = row_off[r];
+      rdesc[r].len = n;
+      rdesc[r].flags = read_uniform[r] ? kReadUniformGaps : 0u;
+    }
+  });
+  if (bad_base.load() >= 0) {
+    char msg[96];
+    snprintf(msg, sizeof(msg), "base 0x%02x is not one of A, C, G, T, N", bad_base.load());
+    return fail(RODV_ERR_INVALID_BASE, msg);
+  }
+
+  // ---- pairs (result order) and per-class lists sorted by haplotype length ----
+  PairDesc* pd = reinterpret_cast<PairDesc*>(s + plan.off_pairs);
+  std::vector<uint64_t> region_off(b.num_regions + 1, 0);
+  for (uint32_t g = 0; g < b.num_regions; ++g)
+    region_off[g + 1] = region_off[g] + (uint64_t)b.regions[g].num_haps * b.regions[g].num_reads;
+  parallel_for(b.num_regions, 64, [&](size_t lo, size_t hi) {
+    for (size_t g = lo; g < hi; ++g) {
+      const rodv_region& rg = b.regions[g];
+      uint64_t p = region_off[g];
+      for (uint32_t h = 0; h < rg.num_haps; ++h)
+        for (uint32_t r = 0; r < rg.num_reads; ++r, ++p) {
+          pd[p].hap = rg.hap_start + h;
+          pd[p].read = rg.read_start + r;
+          pd[p].out = p;
+        }
+    }
+  });
+  // counting sort by (class, hap length descending)
+  const uint32_t nbins = max_h + 1;
+  std::vector<uint32_t> hist((size_t)kNumClasses * nbins, 0);
+  for (uint32_t g = 0; g < b.num_regions; ++g) {
+    const rodv_region& rg = b.regions[g];
+    uint32_t rc[kNumClasses] = {};
+    for (uint32_t r = 0; r < rg.num_reads; ++r) rc[read_class[rg.read_start + r]]++;
+    for (uint32_t h = 0; h < rg.num_haps; ++h) {
+      const uint32_t hl = b.hap_lengths[rg.hap_start + h];
+      for (int c = 0; c < kNumClasses; ++c) hist[(size_t)c * nbins + (max_h - hl)] += rc[c];
+    }
+  }
+  // exclusive prefix per class
+  for (int c = 0; c < kNumClasses; ++c) {
+    uint32_t acc = 0;
+    for (uint32_t k = 0; k < nbins; ++k) {
+      const uint32_t v = hist[(size_t)c * nbins + k];
+      hist[(size_t)c * nbins + k] = acc;
+      acc += v;
+    }
+  }
+  {
+    uint64_t p = 0;
+    for (uint32_t g = 0; g < b.num_regions; ++g) {
+      const rodv_region& rg = b.regions[g];
+      for (uint32_t h = 0; h < rg.num_haps; ++h) {
+        const uint32_t hl = b.hap_lengths[rg.hap_start + h];
+        for (uint32_t r = 0; r < rg.num_reads; ++r, ++p) {
+          const int c = read_class[rg.read_start + r];
+          uint32_t* list = reinterpret_cast<uint32_t*>(s + plan.off_lists[c]);
+          list[hist[(size_t)c * nbins + (max_h - hl)]++] = (uint32_t)p;
+        }
+      }
+    }
+  }
+  // FP32 items: consecutive pairs of the sorted list (longer haplotype first)
+  if (!fp64) {
+    for (int c = 0; c < kNumClasses; ++c) {
+      const uint32_t* list = reinterpret_cast<const uint32_t*>(s + plan.off_lists[c]);
+      Item* it = reinterpret_cast<Item*>(s + plan.off_items[c]);
+      const uint32_t n = plan.pairs[c];
+      for (uint32_t k = 0; k < plan.items[c]; ++k) {
+        it[k].x = list[2 * k];
+        it[k].y = (2 * k + 1 < n) ? list[2 * k + 1] : kNoPair;
+      }
+    }
+  }
+  // cells
+  uint64_t cells = 0;
+  for (uint32_t g = 0; g < b.num_regions; ++g) {
+    const rodv_region& rg = b.regions[g];
+    uint64_t hs = 0, rs = 0;
+    for (uint32_t h = 0; h < rg.num_haps; ++h) hs += b.hap_lengths[rg.hap_start + h];
+    for (uint32_t r = 0; r < rg.num_reads; ++r) rs += b.read_lengths[rg.read_start + r];
+    cells += hs * rs;
+  }
+  plan.cells = cells;
+  return RODV_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Launches
+// ---------------------------------------------------------------------------
+rodv_status Engine::launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stats* st,
+                               bool timed) {
+  ArenaView a = arena_view(plan, dbase, tab_);
+  uint32_t* fp32_ctr = a.counts;
+  uint32_t* fp64_ctr = a.counts + kNumClasses;
+  uint32_t* rescue_cnt = a.counts + 2 * kNumClasses;
+  uint32_t* err = a.counts + 3 * kNumClasses;
+  const bool fp64 = plan.fp64;
+  RODV_CUDA(cudaMemsetAsync(a.counts, 0, kCountWords * 4, stream_));
+  if (fp64) {
+    // every pair goes to the FP64 kernels: the lists are the class lists
+    std::vector<uint32_t> preset(kNumClasses);
+    for (int c = 0; c < kNumClasses; ++c) preset[c] = plan.pairs[c];
+    RODV_CUDA(cudaMemcpyAsync(rescue_cnt, preset.data(), kNumClasses * 4, cudaMemcpyHostToDevice,
+                              stream_));
+  }
+  uint32_t launches = 0;
+  if (timed) RODV_CUDA(cudaEventRecord(ev_[0], stream_));
+  if (!fp64) {
+    for (int c = 0; c < kNumClasses; ++c) {
+      if (!plan.items[c]) continue;
+      const KernelInfo k = forward_kernel_info(Precision::kF32x2, class_rows(c), class_uniform(c),
+                                               class_multi(c));
+      ClassLaunch cl{};
+      cl.work = reinterpret_cast<const uint32_t*>(dbase + plan.off_items[c]);
+      cl.work_count = nullptr;
+      cl.static_count = plan.items[c];
+      cl.counter = fp32_ctr + c;
+      cl.rescue_list = reinterpret_cast<uint32_t*>(dbase + plan.off_lists[c]);
+      cl.rescue_count = rescue_cnt + c;
+      cl.scratch = a.scratch;
+      cl.scratch_cols = plan.scratch_cols;
+      cl.error_flags = err;
+      const int need = (int)((plan.items[c] + k.warps_per_block - 1) / k.warps_per_block);
+      const int blocks = std::max(1, std::min(persistent_blocks(k), need));
+      void* args[] = {&a.view, &cl};
+      RODV_CUDA(cudaLaunchKernel(k.fn, dim3(blocks), dim3(k.threads), args, k.smem_bytes,
+                                 stream_));
+      ++launches;
+    }
+  }
+  if (timed) RODV_CUDA(cudaEventRecord(ev_[1], stream_));
+  for (int c = 0; c < kNumClasses; ++c) {
+    if (!plan.pairs[c]) continue;
+    const KernelInfo k =
+        forward_kernel_info(Precision::kF64, class_rows(c), class_uniform(c), class_multi(c));
+    ClassLaunch cl{};
+    cl.work = reinterpret_cast<const uint32_t*>(dbase + plan.off_lists[c]);
+    cl.work_count = rescue_cnt + c;
+    cl.static_count = 0;
+    cl.counter = fp64_ctr + c;
+    cl.rescue_list = nullptr;
+    cl.rescue_count = nullptr;
+    cl.scratch = a.scratch;
+    cl.scratch_cols = plan.scratch_cols;
+    cl.error_flags = err;
+    const int need = (int)((plan.pairs[c] + k.warps_per_block - 1) / k.warps_per_block);
+    const int blocks = std::max(1, std::min(persistent_blocks(k), need));
+    void* args[] = {&a.view, &cl};
+    RODV_CUDA(cudaLaunchKernel(k.fn, dim3(blocks), dim3(k.threads), args, k.smem_bytes, stream_));
+    ++launches;
+  }
+  if (timed) RODV_CUDA(cudaEventRecord(ev_[2], stream_));
+  if (st) st->kernel_launches += launches;
+  return RODV_OK;
+}
+
+rodv_status Engine::check_errors(const PackedPlan& plan, uint8_t* dbase) {
+  uint32_t tail[kNumClasses + 1];
+  RODV_CUDA(cudaMemcpy(tail, dbase + plan.off_counts + 2 * kNumClasses * 4,
+                       sizeof(tail), cudaMemcpyDeviceToHost));
+  if (tail[kNumClasses] != 0)
+    return fail(RODV_ERR_DEVICE_CHECK,
+                "kernel reported error flags " + std::to_string(tail[kNumClasses]));
+  return RODV_OK;
+}
+
+static void fill_stats(rodv_stats* st, const PackedPlan& plan, const uint32_t* rescue,
+                       bool fp64) {
+  if (!st) return;
+  st->pairs = plan.num_pairs;
+  st->cells = plan.cells;
+  uint64_t n = 0;
+  for (int c = 0; c < kNumClasses; ++c) n += fp64 ? plan.pairs[c] : rescue[c];
+  st->fp64_pairs = n;
+}
+
+rodv_status Engine::run_host(const rodv_batch& b, double* out, rodv_stats* st, bool force_fp64) {
+  if (!out) return fail(RODV_ERR_INVALID_ARG, "null output");
+  const auto t0 = std::chrono::steady_clock::now();
+  RODV_CUDA(cudaSetDevice(device_));
+  PackedPlan plan;
+  rodv_status s = pack(b, plan, staging_, force_fp64 || opt_.force_fp64 != 0);
+  if (s != RODV_OK) return s;
+  RODV_CUDA(arena_.ensure(plan.total_bytes));
+  RODV_CUDA(out_staging_.ensure(plan.num_pairs * 8 + kCountWords * 4));
+  uint8_t* d = static_cast<uint8_t*>(arena_.ptr);
+  RODV_CUDA(cudaEventRecord(ev_[3], stream_));
+  RODV_CUDA(cudaMemcpyAsync(d, staging_.ptr, plan.upload_bytes, cudaMemcpyHostToDevice, stream_));
+  s = launch_all(plan, d, st, true);
+  if (s != RODV_OK) return s;
+  uint8_t* hs = static_cast<uint8_t*>(out_staging_.ptr);
+  RODV_CUDA(cudaMemcpyAsync(hs, d + plan.off_out, plan.num_pairs * 8, cudaMemcpyDeviceToHost,
+                            stream_));
+  RODV_CUDA(cudaMemcpyAsync(hs + plan.num_pairs * 8, d + plan.off_counts, kCountWords * 4,
+                            cudaMemcpyDeviceToHost, stream_));
+  RODV_CUDA(cudaStreamSynchronize(stream_));
+  const uint32_t* counts = reinterpret_cast<const uint32_t*>(hs + plan.num_pairs * 8);
+  if (counts[3 * kNumClasses] != 0)
+    return fail(RODV_ERR_DEVICE_CHECK,
+                "kernel reported error flags " + std::to_string(counts[3 * kNumClasses]));
+  std::memcpy(out, hs, plan.num_pairs * 8);
+  if (st) {
+    fill_stats(st, plan, counts + 2 * kNumClasses, plan.fp64);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev_[0], ev_[2]);
+    st->device_ms = ms;
+    cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+    st->fp32_ms = ms;
+    cudaEventElapsedTime(&ms, ev_[3], ev_[0]);
+    st->h2d_ms = ms;
+    st->h2d_bytes = plan.upload_bytes;
+    st->d2h_bytes = plan.num_pairs * 8 + kCountWords * 4;
+    st->total_ms = ms_since(t0);
+  }
+  return RODV_OK;
+}
+
+rodv_status Engine::upload(const rodv_batch& b, rodv_device_batch** out) {
+  RODV_CUDA(cudaSetDevice(device_));
+  auto* db = new rodv_device_batch();
+  PinnedMem staging;
+  rodv_status s = pack(b, db->plan, staging, opt_.force_fp64 != 0);
+  if (s != RODV_OK) {
+    delete db;
+    return s;
+  }
+  cudaError_t e = db->arena.ensure(db->plan.total_bytes);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(db->arena.ptr, staging.ptr, db->plan.upload_bytes,
+                        cudaMemcpyHostToDevice, stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  if (e != cudaSuccess) {
+    delete db;
+    return cuda_fail(e, "device batch upload");
+  }
+  *out = db;
+  return RODV_OK;
+}
+
+rodv_status Engine::run_device(rodv_device_batch* db, rodv_stats* st) {
+  RODV_CUDA(cudaSetDevice(device_));
+  uint8_t* d = static_cast<uint8_t*>(db->arena.ptr);
+  const auto t0 = std::chrono::steady_clock::now();
+  rodv_status s = launch_all(db->plan, d, st, true);
+  if (s != RODV_OK) return s;
+  RODV_CUDA(cudaStreamSynchronize(stream_));
+  if (st) {
+    uint32_t counts[kCountWords];
+    RODV_CUDA(cudaMemcpy(counts, d + db->plan.off_counts, sizeof(counts),
+                         cudaMemcpyDeviceToHost));
+    fill_stats(st, db->plan, counts + 2 * kNumClasses, db->plan.fp64);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev_[0], ev_[2]);
+    st->device_ms = ms;
+    cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+    st->fp32_ms = ms;
+    st->total_ms = ms_since(t0);
+  }
+  return check_errors(db->plan, d);
+}
+
+rodv_status Engine::download(rodv_device_batch* db, double* out) {
+  RODV_CUDA(cudaSetDevice(device_));
+  RODV_CUDA(cudaMemcpy(out, static_cast<uint8_t*>(db->arena.ptr) + db->plan.off_out,
+                       db->plan.num_pairs * 8, cudaMemcpyDeviceToHost));
+  return RODV_OK;
+}
+
+// The plain GPU form: every pair is its own FP32 launch (one warp, slot y
+// empty), its result is read back, and a pair below 1e-28 gets a second,
+// FP64 launch.  Same kernels as the batched path; no batching.
+rodv_status Engine::plain(rodv_device_batch* db, double* out, rodv_stats* st) {
+  RODV_CUDA(cudaSetDevice(device_));
+  const PackedPlan& plan = db->plan;
+  uint8_t* d = static_cast<uint8_t*>(db->arena.ptr);
+  ArenaView a = arena_view(plan, d, tab_);
+  // scratch words: [0..1] item, [2] pair id, [3] fp32 counter, [4] fp64 counter,
+  // [5] rescue count, [6] rescue list entry, [7] error flags
+  DeviceMem ctl;
+  RODV_CUDA(ctl.ensure(64));
+  uint32_t* w = static_cast<uint32_t*>(ctl.ptr);
+  PinnedMem host;
+  RODV_CUDA(host.ensure(64));
+  uint32_t* hw = static_cast<uint32_t*>(host.ptr);
+  std::vector<PairDesc> pairs(plan.num_pairs);
+  std::vector<ReadDesc> reads(plan.num_reads);
+  RODV_CUDA(cudaMemcpy(pairs.data(), d + plan.off_pairs, plan.num_pairs * sizeof(PairDesc),
+                       cudaMemcpyDeviceToHost));
+  RODV_CUDA(cudaMemcpy(reads.data(), d + plan.off_reads, plan.num_reads * sizeof(ReadDesc),
+                       cudaMemcpyDeviceToHost));
+  uint32_t launches = 0;
+  uint64_t rescued = 0;
+  const auto t0 = std::chrono::steady_clock::now();
+  RODV_CUDA(cudaEventRecord(ev_[0], stream_));
+  for (uint64_t p = 0; p < plan.num_pairs; ++p) {
+    const ReadDesc& rd = reads[pairs[p].read];
+    const int c = class_of(rd.len, (rd.flags & kReadUniformGaps) != 0);
+    hw[0] = (uint32_t)p;
+    hw[1] = kNoPair;
+    hw[2] = (uint32_t)p;
+    hw[3] = hw[4] = hw[5] = hw[6] = hw[7] = 0;
+    RODV_CUDA(cudaMemcpyAsync(w, hw, 32, cudaMemcpyHostToDevice, stream_));
+    for (int pass = 0; pass < 2; ++pass) {
+      const bool f64 = pass == 1 || plan.fp64;
+      const KernelInfo k = forward_kernel_info(f64 ? Precision::kF64 : Precision::kF32x2,
+                                               class_rows(c), class_uniform(c), class_multi(c));
+      ClassLaunch cl{};
+      cl.work = f64 ? w + 2 : w;
+      cl.work_count = nullptr;
+      cl.static_count = 1;
+      cl.counter = f64 ? w + 4 : w + 3;
+      cl.rescue_list = w + 6;
+      cl.rescue_count = w + 5;
+      cl.scratch = a.scratch;
+      cl.scratch_cols = plan.scratch_cols;
+      cl.error_flags = w + 7;
+      void* args[] = {&a.view, &cl};
+      RODV_CUDA(cudaLaunchKernel(k.fn, dim3(1), dim3(k.threads), args, k.smem_bytes, stream_));
+      ++launches;
+      if (f64) break;
+      RODV_CUDA(cudaMemcpyAsync(hw + 5, w + 5, 12, cudaMemcpyDeviceToHost, stream_));
+      RODV_CUDA(cudaStreamSynchronize(stream_));
+      if (hw[7]) return fail(RODV_ERR_DEVICE_CHECK, "plain kernel reported an error");
+      if (hw[5] == 0) break;
+      ++rescued;
+    }
+  }
+  RODV_CUDA(cudaEventRecord(ev_[1], stream_));
+  RODV_CUDA(cudaStreamSynchronize(stream_));
+  if (st) {
+    st->pairs = plan.num_pairs;
+    st->cells = plan.cells;
+    st->fp64_pairs = plan.fp64 ? plan.num_pairs : rescued;
+    st->kernel_launches += launches;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+    st->device_ms = ms;
+    st->total_ms = ms_since(t0);
+  }
+  if (out) return download(db, out);
+  return RODV_OK;
+}
+
+rodv_status Engine::measure_peaks(double* f32, double* f32x2, double* f64, double* mhz) {
+  RODV_CUDA(cudaSetDevice(device_));
+  DeviceMem scratch;
+  RODV_CUDA(scratch.ensure(kPeakScratchBytes));
+  const int threads = 256, blocks = num_sms_ * 8, iters = 4096;
+  double res[3] = {0, 0, 0};
+  double clock_mhz = 0;
+  for (int kind = 0; kind < 3; ++kind) {
+    RODV_CUDA(run_peak(kind, blocks, threads, iters / 8, stream_, scratch.ptr));  // warm-up
+    float best = 1e30f;
+    for (int rep = 0; rep < 5; ++rep) {
+      RODV_CUDA(cudaEventRecord(ev_[0], stream_));
+      RODV_CUDA(run_peak(kind, blocks, threads, iters, stream_, scratch.ptr));
+      RODV_CUDA(cudaEventRecord(ev_[1], stream_));
+      RODV_CUDA(cudaEventSynchronize(ev_[1]));
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+      if (ms < best) {
+        best = ms;
+        if (kind == 0) {
+          long long cyc = 0;
+          RODV_CUDA(cudaMemcpy(&cyc, static_cast<char*>(scratch.ptr) + kPeakCyclesOffset,
+                               sizeof(cyc), cudaMemcpyDeviceToHost));
+          clock_mhz = (double)cyc / (ms * 1e3);
+        }
+      }
+    }
+    res[kind] = peak_flops_per_launch(kind, blocks, threads, iters) / (best * 1e-3) / 1e9;
+  }
+  if (f32) *f32 = res[0];
+  if (f32x2) *f32x2 = res[1];
+  if (f64) *f64 = res[2];
+  if (mhz) *mhz = clock_mhz;
+  return RODV_OK;
+}
+
+}  // namespace rodv

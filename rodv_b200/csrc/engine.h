@@ -1,0 +1,120 @@
+// engine.h -- the engine behind the C ABI (include/rodv_pairhmm.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/rodv_pairhmm.h"
+#include "kernels.h"
+#include "layout.h"
+
+namespace rodv {
+
+// Work classes: single-pass kernels for R = 1..8 rows per lane (reads up to
+// 32*R bases), times {per-row, uniform} gap priors, plus the multi-pass
+// kernels for longer reads.
+constexpr int kSinglePassClasses = kMaxRowsPerLane * 2;
+constexpr int kNumClasses = kSinglePassClasses + 2;
+
+inline int class_of(uint32_t read_len, bool uniform) {
+  if (read_len <= (uint32_t)kPassRows) {
+    const int R = (int)((read_len + kWarp - 1) / kWarp);
+    return (R - 1) * 2 + (uniform ? 1 : 0);
+  }
+  return kSinglePassClasses + (uniform ? 1 : 0);
+}
+inline int class_rows(int cls) { return cls < kSinglePassClasses ? cls / 2 + 1 : kMaxRowsPerLane; }
+inline bool class_uniform(int cls) { return (cls & 1) != 0; }
+inline bool class_multi(int cls) { return cls >= kSinglePassClasses; }
+
+struct DeviceMem {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  ~DeviceMem();
+  cudaError_t ensure(size_t n);
+};
+
+struct PinnedMem {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  ~PinnedMem();
+  cudaError_t ensure(size_t n);
+};
+
+// Host-side description of one packed batch (sizes and per-class counts).
+struct PackedPlan {
+  uint64_t num_pairs = 0, cells = 0;
+  uint64_t hap_code_bytes = 0, read_rows = 0;
+  uint32_t num_haps = 0, num_reads = 0;
+  uint32_t max_hap_len = 0;
+  uint32_t multi_max_hap = 0;
+  uint32_t items[kNumClasses] = {};      // FP32 items (pairs of pairs)
+  uint32_t pairs[kNumClasses] = {};      // pairs per class
+  // byte offsets inside the staging / device arena
+  size_t off_hap_codes = 0, off_read_rows = 0, off_haps = 0, off_reads = 0, off_pairs = 0;
+  size_t off_items[kNumClasses] = {};
+  size_t off_lists[kNumClasses] = {};    // FP64 work lists (rescue or forced)
+  size_t upload_bytes = 0;               // staging part: everything above
+  size_t off_out = 0, off_counts = 0, off_scratch = 0;
+  size_t total_bytes = 0;
+  size_t scratch_bytes = 0;
+  uint32_t scratch_cols = 0;
+  bool fp64 = false;                     // every pair computed in FP64
+};
+
+struct rodv_device_batch_impl;
+
+class Engine {
+ public:
+  explicit Engine(const rodv_options& opt);
+  ~Engine();
+  rodv_status init();
+
+  rodv_status run_host(const rodv_batch& b, double* out, rodv_stats* st, bool force_fp64 = false);
+  rodv_status upload(const rodv_batch& b, rodv_device_batch** out);
+  rodv_status run_device(rodv_device_batch* db, rodv_stats* st);
+  rodv_status download(rodv_device_batch* db, double* out);
+  rodv_status plain(rodv_device_batch* db, double* out, rodv_stats* st);
+  rodv_status measure_peaks(double* f32, double* f32x2, double* f64, double* mhz);
+
+  std::mutex& mutex() { return mu_; }
+  const char* last_error() const { return last_error_.c_str(); }
+  rodv_status fail(rodv_status s, const std::string& msg);
+  rodv_status cuda_fail(cudaError_t e, const char* where);
+
+ private:
+  rodv_status pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64);
+  rodv_status launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stats* st, bool timed);
+  rodv_status check_errors(const PackedPlan& plan, uint8_t* dbase);
+  int persistent_blocks(const KernelInfo& k) const;
+
+  rodv_options opt_;
+  int device_ = 0;
+  int num_sms_ = 0;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev_[4] = {};
+  DeviceMem tables_;
+  PriorTables tab_{};
+  // buffers of the one-call path (rodv_pairhmm_batch), reused across calls
+  PinnedMem staging_;
+  PinnedMem out_staging_;
+  DeviceMem arena_;
+  std::mutex mu_;
+  std::string last_error_;
+  bool ready_ = false;
+};
+
+}  // namespace rodv
+
+// Opaque handles of the C ABI.
+struct rodv_engine {
+  rodv::Engine* impl;
+};
+
+struct rodv_device_batch {
+  rodv::PackedPlan plan;
+  rodv::DeviceMem arena;
+};

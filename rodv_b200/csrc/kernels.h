@@ -1,0 +1,30 @@
+// kernels.h -- host-visible handles to the device kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace rodv {
+
+enum class Precision { kF32x2 = 0, kF64 = 1 };
+
+struct KernelInfo {
+  const void* fn = nullptr;   // __global__ forward_kernel<...>(BatchView, ClassLaunch)
+  int threads = 0;            // threads per block
+  int warps_per_block = 0;
+  int smem_bytes = 0;         // dynamic shared memory per block
+  int rows_per_lane = 0;      // R
+  bool multi = false;         // sweeps reads longer than 32*R rows in passes
+};
+
+// Forward kernel for one work class.  rows_per_lane in 1..8; multi kernels
+// always use 8 rows per lane.
+KernelInfo forward_kernel_info(Precision prec, int rows_per_lane, bool uniform, bool multi);
+
+// Peak microbenchmarks: kind 0 = FP32 FFMA, 1 = FP32x2 FFMA2, 2 = FP64 DFMA.
+// scratch must hold kPeakScratchBytes; the FFMA run stores the SM cycles its
+// first block spent at byte offset kPeakCyclesOffset.
+constexpr int kPeakCyclesOffset = 32768;
+constexpr int kPeakScratchBytes = 65536;
+cudaError_t run_peak(int kind, int blocks, int threads, int iters, cudaStream_t st, void* scratch);
+double peak_flops_per_launch(int kind, int blocks, int threads, int iters);
+
+}  // namespace rodv

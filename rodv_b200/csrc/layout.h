@@ -1,0 +1,112 @@
+// layout.h -- device-side data layout shared by the host packer and kernels.
+//
+// A batch is packed once on the host into these flat arrays (one H2D copy
+// each) and stays resident in HBM while the kernels run:
+//
+//   hap_codes  u8   every haplotype as base codes A0 C1 G2 T3 N4, preceded
+//                   and followed by kHapPad code-0 bytes; the buffer tail
+//                   holds kHapPad + max_hap_len more, so a warp whose shorter
+//                   slot runs past its haplotype end still reads in bounds.
+//   read_rows  u32  one word per read base:
+//                     bits 0-2 base code, 3-9 q, 10-16 ins, 17-23 del,
+//                     24-30 gcp (quals masked with &127 as the reference
+//                     does, pairhmm_inter.cpp:85-88); each read starts on a
+//                     16-byte boundary.
+//   haps       HapDesc[], reads ReadDesc[], pairs PairDesc[]
+//   items      Item[]  the FP32 kernel's work: two pairs per warp (the two
+//                      float lanes of every packed f32x2 instruction)
+//   out        f64[num_pairs]  final log10 likelihood, in the reference's
+//                              result order (region, hap-major, read-minor)
+#pragma once
+#include <cstdint>
+
+namespace rodv {
+
+constexpr int kWarp = 32;
+constexpr int kHapPad = 32;          // code bytes before/after each haplotype
+constexpr int kMaxRowsPerLane = 8;   // R: read rows held in registers per lane
+constexpr int kPassRows = kWarp * kMaxRowsPerLane;  // rows per multi-pass sweep
+constexpr uint32_t kNoPair = 0xffffffffu;
+
+// Base codes.  'N' on either side matches every base (common.h:42-56,
+// pairhmm_impl.cpp:26-42).
+enum BaseCode : uint8_t { kA = 0, kC = 1, kG = 2, kT = 3, kN = 4 };
+
+struct HapDesc {
+  uint64_t code_off;  // index in hap_codes of the first base
+  uint32_t len;
+  uint32_t pad_;
+};
+
+struct ReadDesc {
+  uint64_t row_off;   // index in read_rows of the first row word
+  uint32_t len;
+  uint32_t flags;     // kReadUniformGaps: ins, del and gcp constant over the read
+};
+constexpr uint32_t kReadUniformGaps = 1u;
+
+struct PairDesc {
+  uint32_t hap;
+  uint32_t read;
+  uint64_t out;       // index in the output array
+};
+
+// Two pairs computed together by one warp.  Slot x is the pair with the
+// longer (or equal) haplotype; y may be kNoPair.
+struct Item {
+  uint32_t x;
+  uint32_t y;
+};
+
+__host__ __device__ inline uint32_t row_word(uint32_t code, uint32_t q, uint32_t ins,
+                                             uint32_t del, uint32_t gcp) {
+  return (code & 7u) | ((q & 127u) << 3) | ((ins & 127u) << 10) | ((del & 127u) << 17) |
+         ((gcp & 127u) << 24);
+}
+__host__ __device__ inline uint32_t rw_code(uint32_t w) { return w & 7u; }
+__host__ __device__ inline uint32_t rw_q(uint32_t w) { return (w >> 3) & 127u; }
+__host__ __device__ inline uint32_t rw_ins(uint32_t w) { return (w >> 10) & 127u; }
+__host__ __device__ inline uint32_t rw_del(uint32_t w) { return (w >> 17) & 127u; }
+__host__ __device__ inline uint32_t rw_gcp(uint32_t w) { return (w >> 24) & 127u; }
+
+// Prior tables in the two precisions (Context<float>/Context<double>,
+// context.h:22-166): ph2pr[q] and the match-to-match table indexed by
+// (max*(max+1))/2 + min of the (ins, del) quals.
+constexpr int kMmTableSize = 128 * 129 / 2;
+struct PriorTables {
+  const float* ph2pr_f;
+  const float* mm_f;
+  const double* ph2pr_d;
+  const double* mm_d;
+};
+
+// Everything a forward kernel needs about the resident batch.
+struct BatchView {
+  const uint8_t* hap_codes;
+  const uint32_t* read_rows;
+  const HapDesc* haps;
+  const ReadDesc* reads;
+  const PairDesc* pairs;
+  double* out;
+  PriorTables tab;
+};
+
+// One launch of a forward kernel over one class of work.
+struct ClassLaunch {
+  const uint32_t* work;        // FP32: Item list (2 words per item); FP64: pair list
+  const uint32_t* work_count;  // device count (FP64 rescue lists) or null
+  uint32_t static_count;       // item count when work_count is null
+  uint32_t* counter;           // work counter, zeroed before launch
+  uint32_t* rescue_list;       // FP32 only: pairs whose result fell below 1e-28
+  uint32_t* rescue_count;
+  float* scratch;              // MULTI: per resident warp boundary-row buffer
+  uint32_t scratch_cols;       // columns per warp buffer (max hap len + 40)
+  uint32_t* error_flags;       // bit set by a kernel that hit a bad descriptor
+};
+
+enum ErrorFlag : uint32_t {
+  kErrBadLength = 1u,   // a pair with zero or over-limit length reached a kernel
+  kErrPassLimit = 2u,   // a read longer than the pass limit reached a kernel
+};
+
+}  // namespace rodv

@@ -1,0 +1,123 @@
+// pairhmm_kernels.cu -- instantiations of the forward kernels, their dispatch
+// table, and the arithmetic-peak microbenchmarks used as roofline
+// denominators.
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+#include "pairhmm_fwd.cuh"
+
+namespace rodv {
+
+namespace {
+
+template <class P, int R, bool U, bool MU>
+KernelInfo info_of() {
+  KernelInfo k;
+  k.fn = reinterpret_cast<const void*>(&forward_kernel<P, R, U, MU>);
+  k.threads = Forward<P, R, U, MU>::kWarpsPerBlock * kWarp;
+  k.warps_per_block = Forward<P, R, U, MU>::kWarpsPerBlock;
+  k.smem_bytes = Forward<P, R, U, MU>::kWarpsPerBlock * TableShape<P, R>::kBytesPerWarp;
+  k.rows_per_lane = R;
+  k.multi = MU;
+  return k;
+}
+
+template <class P, bool U>
+KernelInfo single_pass(int R) {
+  switch (R) {
+    case 1: return info_of<P, 1, U, false>();
+    case 2: return info_of<P, 2, U, false>();
+    case 3: return info_of<P, 3, U, false>();
+    case 4: return info_of<P, 4, U, false>();
+    case 5: return info_of<P, 5, U, false>();
+    case 6: return info_of<P, 6, U, false>();
+    case 7: return info_of<P, 7, U, false>();
+    default: return info_of<P, 8, U, false>();
+  }
+}
+
+}  // namespace
+
+KernelInfo forward_kernel_info(Precision prec, int rows_per_lane, bool uniform, bool multi) {
+  if (prec == Precision::kF32x2) {
+    if (multi) return uniform ? info_of<F32x2, kMaxRowsPerLane, true, true>()
+                              : info_of<F32x2, kMaxRowsPerLane, false, true>();
+    return uniform ? single_pass<F32x2, true>(rows_per_lane)
+                   : single_pass<F32x2, false>(rows_per_lane);
+  }
+  if (multi) return uniform ? info_of<F64, kMaxRowsPerLane, true, true>()
+                            : info_of<F64, kMaxRowsPerLane, false, true>();
+  return uniform ? single_pass<F64, true>(rows_per_lane) : single_pass<F64, false>(rows_per_lane);
+}
+
+// ---- arithmetic-peak microbenchmarks (measurement only) -------------------
+// Each thread runs kChains independent dependency chains so that every SM
+// sub-partition always has an FMA ready; values stay normal and bounded.
+constexpr int kChains = 8;
+
+__global__ void peak_ffma_kernel(float* out, int iters, float b, float c, long long* cycles) {
+  const long long t0 = clock64();
+  float a[kChains];
+#pragma unroll
+  for (int k = 0; k < kChains; ++k) a[k] = 1.0f + 0.001f * (threadIdx.x + k);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int k = 0; k < kChains; ++k) a[k] = fmaf(a[k], b, c);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < kChains; ++k) s += a[k];
+  if (s == 12345.678f) out[threadIdx.x] = s;  // keeps the chains alive
+  if (threadIdx.x == 0 && blockIdx.x == 0) *cycles = clock64() - t0;
+}
+
+__global__ void peak_ffma2_kernel(float* out, int iters, float b, float c) {
+  float2 a[kChains];
+  const float2 bb = make_float2(b, b), cc = make_float2(c, c);
+#pragma unroll
+  for (int k = 0; k < kChains; ++k)
+    a[k] = make_float2(1.0f + 0.001f * (threadIdx.x + k), 1.0f - 0.001f * k);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int k = 0; k < kChains; ++k) a[k] = __ffma2_rn(a[k], bb, cc);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < kChains; ++k) s += a[k].x + a[k].y;
+  if (s == 12345.678f) out[threadIdx.x] = s;
+}
+
+__global__ void peak_dfma_kernel(double* out, int iters, double b, double c) {
+  double a[kChains];
+#pragma unroll
+  for (int k = 0; k < kChains; ++k) a[k] = 1.0 + 0.001 * (threadIdx.x + k);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int k = 0; k < kChains; ++k) a[k] = fma(a[k], b, c);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < kChains; ++k) s += a[k];
+  if (s == 12345.678) out[threadIdx.x] = s;
+}
+
+cudaError_t run_peak(int kind, int blocks, int threads, int iters, cudaStream_t st,
+                     void* scratch) {
+  const float b = 0.9999999f, c = 1e-7f;
+  long long* cycles = reinterpret_cast<long long*>(static_cast<char*>(scratch) + kPeakCyclesOffset);
+  switch (kind) {
+    case 0:
+      peak_ffma_kernel<<<blocks, threads, 0, st>>>((float*)scratch, iters, b, c, cycles);
+      break;
+    case 1: peak_ffma2_kernel<<<blocks, threads, 0, st>>>((float*)scratch, iters, b, c); break;
+    default: peak_dfma_kernel<<<blocks, threads, 0, st>>>((double*)scratch, iters, 0.9999999, 1e-7);
+  }
+  return cudaGetLastError();
+}
+
+double peak_flops_per_launch(int kind, int blocks, int threads, int iters) {
+  const double per_fma = (kind == 1) ? 4.0 : 2.0;  // f32x2 FMA = 2 FMAs = 4 flops
+  return per_fma * kChains * (double)iters * blocks * threads;
+}
+
+}  // namespace rodv

@@ -1,0 +1,227 @@
+"""GPU parity: the engine (through the C ABI) against the oracle and the reference.
+
+Tolerance: |delta log10| <= 1e-3 is the engine's contract; these tests use the
+reference's own test tolerance (1e-5 absolute, pairhmm_unittest.cpp and
+pairhmm_schedule_unittest.cpp) wherever the oracle runs the same precision
+path, and 1e-3 only where noted.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import assemble_batch, synthetic_batch
+from rodv_b200 import RodvError, TestCase, compute_likelihoods, schedule_pairhmm, workloads
+from rodv_b200.batch import Batch
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5          # same-path tolerance (reference tests' abs 1e-5)
+CONTRACT = 1e-3     # engine contract in log10 units
+
+
+def test_simple_known_answers(engine):
+    q4 = [43] * 4
+    assert abs(engine.pair("ACGT", "ACGT", q4, q4, q4, q4) - (-6.022797e-01)) < TOL
+    q5 = [43] * 5
+    assert abs(engine.pair("ACGTA", "ACGTA", q5, q5, q5, q5) - (-0.69925308227539062)) < TOL
+    assert abs(engine.pair("ACGTA", "ACGTA", q5, q5, q5, q5, use_double=True) -
+               (-0.69925308227539062)) < TOL
+
+
+def test_golden_file_one_pair_at_a_time(engine, gkl_cases):
+    for hap, read, q, i, d, c, expected, ref_f, ref_d in gkl_cases[:40]:
+        got = engine.pair(hap, read, q, i, d, c)
+        assert abs(got - expected) / abs(expected) < 1e-5
+        assert abs(got - ref_f) < TOL
+        got_d = engine.pair(hap, read, q, i, d, c, use_double=True)
+        assert abs(got_d - ref_d) < 1e-9
+
+
+def test_golden_file_as_one_batch(engine, gkl_cases):
+    """All 104 golden cases as single-pair regions of one batch (the inter tests' shape)."""
+    regions = [([hap], [read], [q], [i], [d], [c]) for hap, read, q, i, d, c, *_ in gkl_cases]
+    b = Batch.from_regions(regions)
+    got = engine.batch(b)
+    exp = np.array([x[6] for x in gkl_cases])
+    ref = np.array([x[7] for x in gkl_cases])
+    assert np.all(np.abs(got - exp) / np.abs(exp) < 1e-5)
+    assert np.abs(got - ref).max() < TOL
+    got_d = engine.batch(b, use_double=True)
+    ref_d = np.array([x[8] for x in gkl_cases])
+    assert np.abs(got_d - ref_d).max() < 1e-9
+
+
+def test_assemble_regions_match_reference(engine):
+    b, ref = assemble_batch()
+    got, st = engine.batch(b, stats=True)
+    assert st["pairs"] == len(ref)
+    assert np.abs(got - ref).max() < TOL
+    assert np.abs(got - oracle.batch_log10(b)).max() < TOL
+
+
+def test_synthetic_n_bases_and_per_row_quals(engine):
+    b, sched, intra = synthetic_batch()
+    got = engine.batch(b)
+    assert np.abs(got - intra).max() < TOL
+    assert np.abs(got - sched).max() < TOL
+
+
+@pytest.mark.parametrize("name,scale", [("tiny", 4.0), ("plain", 1.0), ("uneven", 0.01),
+                                        ("stream", 0.02)])
+def test_workloads_match_oracle(engine, name, scale):
+    b = workloads.make_workload(name, scale=scale)
+    got, st = engine.batch(b, stats=True)
+    ref = oracle.batch_log10(b)
+    assert np.isfinite(got).all()
+    assert np.abs(got - ref).max() < TOL, (name, np.abs(got - ref).max())
+    true = oracle.batch_log10(b, oracle.SCALED)
+    assert np.abs(got - true).max() < CONTRACT
+
+
+def test_underflow_sample_rescued_in_fp64(engine):
+    b = workloads.make_workload("underflow", scale=0.002)
+    got, st = engine.batch(b, stats=True)
+    assert st["fp64_pairs"] == b.num_pairs  # every FP32 result falls below 1e-28
+    ref = oracle.batch_log10(b, oracle.FP64)
+    assert np.abs(got - ref).max() < 1e-9
+    true = oracle.batch_log10(b, oracle.SCALED)
+    assert np.abs(got - true).max() < CONTRACT
+
+
+def test_long_pairs_multi_pass(engine):
+    b = workloads.make_workload("long", scale=0.004)  # 8 pairs of 1-2 kb reads x 2-5 kb haps
+    got = engine.batch(b)
+    ref = oracle.batch_log10(b, oracle.REFERENCE)
+    finite = np.isfinite(ref)
+    assert np.abs(got[finite] - ref[finite]).max() < TOL
+
+
+def test_multi_pass_fp32_path():
+    """Reads longer than one pass that stay in FP32 range (high identity)."""
+    from rodv_b200 import Engine
+    e = Engine(0)
+    rng = np.random.default_rng(11)
+    regs = []
+    for L in (257, 300, 511, 512, 513, 800):
+        hap = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, L + 40)]
+        read = hap[20:20 + L].copy()
+        q = rng.integers(30, 41, L).astype(np.uint8)
+        regs.append(([hap], [read], [q], [np.full(L, 45, np.uint8)],
+                     [np.full(L, 45, np.uint8)], [np.full(L, 10, np.uint8)]))
+        # per-row gap quals too
+        regs.append(([hap], [read], [q], [rng.integers(30, 50, L).astype(np.uint8)],
+                     [rng.integers(30, 50, L).astype(np.uint8)],
+                     [rng.integers(5, 20, L).astype(np.uint8)]))
+    b = Batch.from_regions(regs)
+    got, st = e.batch(b, stats=True)
+    ref = oracle.batch_log10(b)
+    assert st["fp64_pairs"] < b.num_pairs
+    assert np.abs(got - ref).max() < TOL
+    e.close()
+
+
+def test_edge_lengths(engine):
+    """Reads of 1 base, reads longer than the haplotype, one-base haplotypes,
+    every rows-per-lane class boundary (32*R and 32*R+1), odd pair counts."""
+    rng = np.random.default_rng(7)
+    regs = []
+    for L in (1, 2, 31, 32, 33, 63, 64, 65, 96, 97, 128, 129, 160, 192, 224, 255, 256):
+        for H in (1, 5, L + 3, 2 * L + 1):
+            hap = np.frombuffer(b"ACGTN", np.uint8)[rng.integers(0, 4, H)]
+            read = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, L)]
+            regs.append(([hap], [read], [rng.integers(6, 44, L).astype(np.uint8)],
+                         [rng.integers(6, 44, L).astype(np.uint8)],
+                         [rng.integers(6, 44, L).astype(np.uint8)],
+                         [rng.integers(6, 44, L).astype(np.uint8)]))
+    b = Batch.from_regions(regs)
+    got = engine.batch(b)
+    ref = oracle.batch_log10(b)
+    assert np.abs(got - ref).max() < TOL
+
+
+def test_gap_qual_extremes(engine):
+    """gcp quality 0 (gap continuation probability 1) and ins/del quality 0."""
+    rng = np.random.default_rng(9)
+    regs = []
+    for gq, iq in ((0, 45), (1, 45), (10, 0), (127, 127), (255, 200)):
+        L, H = 40, 60
+        hap = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, H)]
+        read = hap[5:5 + L].copy()
+        regs.append(([hap], [read], [rng.integers(10, 40, L).astype(np.uint8)],
+                     [np.full(L, iq, np.uint8)], [np.full(L, iq, np.uint8)],
+                     [np.full(L, gq, np.uint8)]))
+    b = Batch.from_regions(regs)
+    got = engine.batch(b)
+    ref = oracle.batch_log10(b)
+    ok = np.isfinite(ref)
+    assert np.array_equal(np.isfinite(got), ok)
+    assert np.abs(got[ok] - ref[ok]).max() < TOL
+
+
+def test_force_fp64_matches_fp64_oracle(engine):
+    b = workloads.make_workload("tiny", scale=2.0)
+    got, st = engine.batch(b, use_double=True, stats=True)
+    assert st["fp64_pairs"] == b.num_pairs
+    assert np.abs(got - oracle.batch_log10(b, oracle.FP64)).max() < 1e-9
+
+
+def test_device_batch_reruns_are_identical(engine):
+    b = workloads.make_workload("uneven", scale=0.002)
+    db = engine.upload(b)
+    db.run()
+    first = db.download()
+    db.run()
+    second = db.download()
+    assert np.array_equal(first, second)
+    assert np.abs(first - engine.batch(b)).max() == 0.0
+    db.free()
+
+
+def test_plain_form_matches_batched(engine):
+    b = workloads.make_workload("tiny", scale=1.0)
+    db = engine.upload(b)
+    got, st = engine.plain(db)
+    assert st["kernel_launches"] >= b.num_pairs
+    assert np.abs(got - oracle.batch_log10(b)).max() < TOL
+    db.free()
+
+
+def test_schedule_pairhmm_mirror():
+    b = workloads.make_workload("tiny", scale=1.0)
+    haps, reads, q, i, d, c = b.region(0)
+    result = []
+    assert schedule_pairhmm(haps, reads, result, q, i, d, c)
+    assert len(result) == len(haps) and all(len(r) == len(reads) for r in result)
+    flat = np.array(result).ravel()
+    assert np.abs(flat - oracle.batch_log10(b.subset([0]))).max() < TOL
+    assert schedule_pairhmm([], reads, result, q, i, d, c) is False
+    assert schedule_pairhmm(haps, [], result, [], [], [], []) is False
+
+
+def test_compute_likelihoods_mirror(gkl_cases):
+    hap, read, q, i, d, c, expected, *_ = gkl_cases[0]
+    tc = TestCase(hap, read, q, i, d, c)
+    assert abs(compute_likelihoods(tc) - expected) / abs(expected) < 1e-5
+    assert abs(compute_likelihoods(tc, use_double=True) - expected) / abs(expected) < 1e-5
+
+
+def test_invalid_inputs_fail_loudly(engine):
+    good = ([b"ACGT"], [b"ACG"], [[30] * 3], [[45] * 3], [[45] * 3], [[10] * 3])
+    with pytest.raises(RodvError) as ei:
+        engine.batch(Batch.from_regions([([b"ACGU"],) + good[1:]]))
+    assert ei.value.status == 3
+    with pytest.raises(RodvError) as ei:
+        engine.batch(Batch.from_regions([(good[0], [b"acg"]) + good[2:]]))
+    assert ei.value.status == 3
+    with pytest.raises(RodvError) as ei:
+        engine.batch(Batch.from_regions([([], ) + good[1:]]))
+    assert ei.value.status == 2
+    with pytest.raises(RodvError) as ei:
+        engine.batch(Batch.from_regions([([b""],) + good[1:]]))
+    assert ei.value.status == 1
+    # the engine stays usable after rejected calls
+    assert np.isfinite(engine.batch(Batch.from_regions([good]))).all()
+
+
+def test_peaks_are_measured(engine):
+    p = engine.measure_peaks()
+    assert p["fp32_gflops"] > 1e4 and p["fp64_gflops"] > 1e3 and p["sm_mhz"] > 300
