@@ -134,6 +134,13 @@ def reference_rate(batch, threads: int):
     return batch.cells() / dt / 1e9, dt
 
 
+def sized_sample(name: str, seed: int, seconds: float, threads: int):
+    """A seeded sample sized, from a short probe run, to take about `seconds`."""
+    probe = sample_for_cpu(name, seed + 1, 2e9)
+    rate, _ = reference_rate(probe, threads)  # also warms the reference's tables
+    return sample_for_cpu(name, seed, rate * 1e9 * seconds)
+
+
 def sample_for_cpu(name: str, seed: int, target_cells: float):
     """A seeded prefix of the workload holding about target_cells cells."""
     from rodv_b200 import workloads
@@ -158,10 +165,9 @@ def run_reference(args, world, rank):
                           "oracle/_ref/libref_pairhmm.so was not built (reference tree absent "
                           "at build time)"}))
         return
-    # ~2e10 cells per step keeps K+W steps within a few minutes on ~8-64 cores
-    target = args.ref_cells_per_step
-    batch = sample_for_cpu(args.workload, 7000, target)
-    warm = sample_for_cpu(args.workload, 7001, target / 20)
+    # each step is a sample sized to take about --ref-seconds on all host cores
+    batch = sized_sample(args.workload, 7000, args.ref_seconds, threads)
+    warm = sample_for_cpu(args.workload, 7002, batch.cells() / 10)
     for _ in range(max(1, args.warmup)):
         reference_rate(warm, threads)
     times = []
@@ -339,9 +345,7 @@ def cpu_baseline(args):
         return {"value": None, "unit": "GCUPS", "cores": 0, "kind": "reference",
                 "sample": "unavailable: oracle/_ref was not built"}
     threads = os.cpu_count() or 1
-    batch = sample_for_cpu(args.workload, 7000, args.ref_cells_per_step)
-    warm = sample_for_cpu(args.workload, 7001, args.ref_cells_per_step / 20)
-    reference_rate(warm, threads)
+    batch = sized_sample(args.workload, 7000, args.cpu_seconds, threads)
     rate, dt = reference_rate(batch, threads)
     return {"value": rate, "unit": "GCUPS", "cores": threads, "kind": "reference",
             "sample": f"{batch.num_regions} regions / {batch.num_pairs} pairs / "
@@ -361,7 +365,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--plain-pairs", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-cells-per-step", type=float, default=2e10)
+    ap.add_argument("--ref-seconds", type=float, default=6.0,
+                    help="reference arm: wall seconds of CPU work per step")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="cpu_baseline: wall seconds of CPU work")
     args = ap.parse_args()
     world, rank, local = dist_env()
     if args.impl == "reference":

@@ -46,6 +46,7 @@
 // gapm*sum(M~) + sum(I).
 #pragma once
 #include <cuda_runtime.h>
+#include <math_constants.h>
 #include <stdint.h>
 
 #include "layout.h"
@@ -59,6 +60,7 @@ constexpr float kMinAcceptedF = 1e-28f;
 // literal, promoted to double for the FP64 log10 conversion.
 constexpr double kLog10InitF = (double)36.1236000061f;
 constexpr double kLog10InitD = 307.050595577260822;
+constexpr double kDblMin = 2.2250738585072014e-308;  // smallest normal double
 
 struct F32x2 {
   using V = float2;
@@ -386,7 +388,11 @@ __device__ void Forward<P, R, UNIFORM, MULTI>::finish(const BatchView& b, const 
       c.rescue_list[k] = sl.pair;
     }
   } else {
-    b.out[sl.out] = log10((double)raw) - kLog10InitD;
+    // The reference computes with flush-to-zero on (common.h:58-62), which on
+    // x86 also flushes FP64 denormals: a likelihood below the normal FP64
+    // range of the 2^1020 scaling becomes 0 and its log10 is -inf.  The GPU's
+    // FP64 keeps denormals, so such a result is mapped to -inf here.
+    b.out[sl.out] = (raw >= kDblMin) ? log10((double)raw) - kLog10InitD : -CUDART_INF;
   }
 }
 
