@@ -161,6 +161,37 @@ rodv_status rodv_pairhmm_plain(rodv_engine* engine, rodv_device_batch* dbatch,
 rodv_status rodv_measure_peaks(rodv_engine* engine, double* fp32_gflops, double* fp32x2_gflops,
                                double* fp64_gflops, double* sm_mhz);
 
+/* ---- Allocation-free batch call ------------------------------------------
+ * No counterpart in the reference (roDV computes on the CPU and allocates per
+ * call).  For callers that cannot call cudaMalloc: code that owns all device
+ * memory through its own allocator or a pool reserved at start-up, or that
+ * runs where an allocation would synchronise the device or may fail.  The
+ * caller allocates the inputs and the output its own way; this call
+ * allocates nothing (no cudaMalloc, cudaFree or cudaMallocHost).  Its
+ * scratch is one fixed array of about 12 MB in the library's device memory,
+ * held by every GPU that loads the library until the process exits.
+ *
+ * batch: a rodv_batch whose array pointers (regions included) are DEVICE
+ * memory on the current device; out_log10: device array of
+ * rodv_batch_num_pairs() doubles; stream: a cudaStream_t (NULL = default).
+ * Same results as rodv_pairhmm_batch (every pair through the per-row-prior
+ * multi-pass kernels).  Returns after the work on `stream` has finished.
+ * The first call on a device sets that device up (obtains the scratch
+ * address, copies the prior tables) and synchronises it: make it before any
+ * stream capture.  All calls in a process share the scratch array: calls
+ * that overlap on the GPU race and must be serialised by the caller.
+ * Sizes beyond the limits below return RODV_ERR_TOO_LONG; on any error the
+ * output contents are unspecified. */
+#define RODV_NOALLOC_MAX_REGIONS 4096u
+#define RODV_NOALLOC_MAX_HAPS 4096u
+#define RODV_NOALLOC_MAX_READS 16384u
+#define RODV_NOALLOC_MAX_PAIRS 16384u
+#define RODV_NOALLOC_MAX_HAP_LEN 2048u      /* bases per haplotype */
+#define RODV_NOALLOC_MAX_HAP_BASES 1048576u /* bases over all haplotypes */
+#define RODV_NOALLOC_MAX_READ_BASES 1048576u /* bases over all reads */
+rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32_t use_double,
+                                       double* out_log10, void* stream);
+
 /* Human-readable name of a status code (static storage). */
 const char* rodv_status_string(rodv_status status);
 

@@ -86,6 +86,8 @@ SIGNATURES = [
     ("rodv_pairhmm_plain", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, _f64p,
                                             ctypes.POINTER(Stats)]),
     ("rodv_measure_peaks", ctypes.c_int32, [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p]),
+    ("rodv_pairhmm_batch_noalloc", ctypes.c_int32, [ctypes.POINTER(CBatch), ctypes.c_int32,
+                                                    ctypes.c_void_p, ctypes.c_void_p]),
     ("rodv_status_string", ctypes.c_char_p, [ctypes.c_int32]),
     ("rodv_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
 ]
