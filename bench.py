@@ -319,6 +319,30 @@ def run_engine(args, world, rank, local):
     eng.close()
 
 
+def run_profile(args, local):
+    """--mode profile: upload the workload, W untimed + K timed resident steps,
+    nothing else launched (the command that ncu captures)."""
+    from rodv_b200 import Engine, workloads
+    batch = workloads.make_workload(args.workload, seed=workloads.SEEDS[args.workload],
+                                    scale=args.scale)
+    eng = Engine(local)
+    db = eng.upload(batch)
+    for _ in range(args.warmup):
+        db.run()
+    stats = [db.run() for _ in range(args.steps)]
+    db.free()
+    cells = batch.cells()
+    dev = sum(s["device_ms"] for s in stats) / max(1, len(stats))
+    fp32 = sum(s["fp32_ms"] for s in stats) / max(1, len(stats))
+    print(json.dumps({"mode": "profile", "workload": args.workload, "scale": args.scale,
+                      "pairs": batch.num_pairs, "cells": cells, "device_ms": dev,
+                      "fp32_ms": fp32, "gcups": cells / dev / 1e6 if dev else None,
+                      "fp64_pairs": stats[-1]["fp64_pairs"] if stats else None,
+                      "launches_per_step": stats[-1]["kernel_launches"] if stats else None}),
+          flush=True)
+    eng.close()
+
+
 def plain_form(eng, args):
     """Plain one-pair-per-launch GPU form vs the batched engine on one sample."""
     from rodv_b200 import workloads
@@ -357,9 +381,11 @@ def cpu_baseline(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["rodv", "reference"], default="rodv")
+    ap.add_argument("--mode", choices=["bench", "profile"], default="bench",
+                    help="profile: resident steps only, for ncu captures")
     ap.add_argument("--workload", default="uneven")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -371,7 +397,9 @@ def main():
                     help="cpu_baseline: wall seconds of CPU work")
     args = ap.parse_args()
     world, rank, local = dist_env()
-    if args.impl == "reference":
+    if args.mode == "profile":
+        run_profile(args, local)
+    elif args.impl == "reference":
         run_reference(args, world, rank)
     else:
         run_engine(args, world, rank, local)

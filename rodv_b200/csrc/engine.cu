@@ -706,13 +706,17 @@ rodv_status Engine::measure_peaks(double* f32, double* f32x2, double* f64, doubl
   RODV_CUDA(cudaSetDevice(device_));
   DeviceMem scratch;
   RODV_CUDA(scratch.ensure(kPeakScratchBytes));
-  const int threads = 256, blocks = num_sms_ * 8, iters = 4096;
+  // 8 blocks of 256 threads per SM (all resident); ~20-40 ms per launch
+  const int threads = 256, blocks = num_sms_ * 8, iters = 262144;
   double res[3] = {0, 0, 0};
   double clock_mhz = 0;
   for (int kind = 0; kind < 3; ++kind) {
     RODV_CUDA(run_peak(kind, blocks, threads, iters / 8, stream_, scratch.ptr));  // warm-up
     float best = 1e30f;
-    for (int rep = 0; rep < 5; ++rep) {
+    for (int rep = 0; rep < 3; ++rep) {
+      if (kind == 0)
+        RODV_CUDA(cudaMemsetAsync(static_cast<char*>(scratch.ptr) + kPeakCyclesOffset, 0, 8,
+                                  stream_));
       RODV_CUDA(cudaEventRecord(ev_[0], stream_));
       RODV_CUDA(run_peak(kind, blocks, threads, iters, stream_, scratch.ptr));
       RODV_CUDA(cudaEventRecord(ev_[1], stream_));
