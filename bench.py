@@ -222,6 +222,9 @@ def run_engine(args, world, rank, local):
         log(f"workload {args.workload}: {batch.num_regions} regions, {batch.num_pairs} pairs, "
             f"{cells:.3e} cells (generated in {time.perf_counter() - t_gen:.1f} s)")
     eng = Engine(local)
+    t_tune = time.perf_counter()
+    variants = eng.autotune()
+    t_tune = time.perf_counter() - t_tune
     peaks = eng.measure_peaks()
     db = eng.upload(batch)
 
@@ -284,7 +287,8 @@ def run_engine(args, world, rank, local):
                        "pairs": batch.num_pairs, "cells": cells, "scale": args.scale,
                        "l2": "inputs larger than L2 (resident batch ~%.2f GB)" %
                              (batch.input_bytes() / 1e9),
-                       "parallelism": f"dp{world} (regions sharded, no collective)"},
+                       "parallelism": f"dp{world} (regions sharded, no collective)",
+                       "tuned_variants": variants, "tune_s": round(t_tune, 2)},
             "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": len(e2e_ms),
                     "ms_per_step": e2e_total / len(e2e_ms) * 1e3,
@@ -326,6 +330,8 @@ def run_profile(args, local):
     batch = workloads.make_workload(args.workload, seed=workloads.SEEDS[args.workload],
                                     scale=args.scale)
     eng = Engine(local)
+    if args.tune:
+        eng.autotune()
     db = eng.upload(batch)
     for _ in range(args.warmup):
         db.run()
@@ -391,6 +397,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--plain-pairs", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune", action="store_true", help="profile mode: autotune first")
     ap.add_argument("--ref-seconds", type=float, default=6.0,
                     help="reference arm: wall seconds of CPU work per step")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,

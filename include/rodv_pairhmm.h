@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define RODV_ABI_VERSION 1
+#define RODV_ABI_VERSION 2
 
 typedef int32_t rodv_status;
 enum {
@@ -92,6 +92,10 @@ typedef struct rodv_options {
   uint64_t device_memory_budget;/* bytes the streaming service may hold; 0 = 50% of free */
   uint32_t max_inflight;        /* streaming: regions admitted at once; 0 = 4096 */
   int32_t verbose;              /* 1: print per-batch statistics to stderr */
+  int32_t autotune;             /* 0: cached or default kernel variants; 1: tune at creation
+                                   unless the cache has this device; 2: always tune */
+  const char* tune_cache;       /* file of tuned variants (read, and written after tuning);
+                                   NULL = none */
 } rodv_options;
 
 typedef struct rodv_stats {
@@ -191,6 +195,16 @@ rodv_status rodv_measure_peaks(rodv_engine* engine, double* fp32_gflops, double*
 #define RODV_NOALLOC_MAX_READ_BASES 1048576u /* bases over all reads */
 rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32_t use_double,
                                        double* out_log10, void* stream);
+
+/* Autotuner: per work class (read-length bucket and gap-prior form), times
+ * every occupancy variant (register budget) of the FP32 kernel on a synthetic
+ * batch of that class and keeps the fastest.  With cache_path, a cached
+ * result for this device is used unless force != 0, and new results are
+ * written there.  variants_out (may be NULL) receives RODV_TUNE_CLASSES
+ * variant indices. */
+#define RODV_TUNE_CLASSES 18
+rodv_status rodv_autotune(rodv_engine* engine, const char* cache_path, int32_t force,
+                          int32_t* variants_out);
 
 /* Human-readable name of a status code (static storage). */
 const char* rodv_status_string(rodv_status status);

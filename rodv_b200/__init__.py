@@ -84,7 +84,8 @@ class Engine:
     """A PairHMM engine on one CUDA device (rodv_engine)."""
 
     def __init__(self, device: int = 0, force_fp64: bool = False, verbose: bool = False,
-                 device_memory_budget: int = 0, max_inflight: int = 0):
+                 device_memory_budget: int = 0, max_inflight: int = 0, autotune: int = 0,
+                 tune_cache: Optional[str] = None):
         self.lib = _lib.load()
         opts = _lib.Options()
         self.lib.rodv_default_options(ctypes.byref(opts))
@@ -93,6 +94,9 @@ class Engine:
         opts.verbose = int(verbose)
         opts.device_memory_budget = device_memory_budget
         opts.max_inflight = max_inflight
+        opts.autotune = autotune
+        self._tune_cache = tune_cache.encode() if tune_cache else None
+        opts.tune_cache = self._tune_cache
         h = ctypes.c_void_p()
         st = self.lib.rodv_engine_create(ctypes.byref(opts), ctypes.byref(h))
         if st != _lib.RODV_OK:
@@ -159,6 +163,13 @@ class Engine:
         self._check(self.lib.rodv_pairhmm_plain(self.h, db.handle, _ptr(out, _lib._f64p),
                                                 ctypes.byref(st)))
         return out, st.as_dict()
+
+    def autotune(self, cache_path: Optional[str] = None, force: bool = False) -> List[int]:
+        """Tunes the FP32 kernel's occupancy variant per work class; returns them."""
+        v = (ctypes.c_int32 * 18)()
+        self._check(self.lib.rodv_autotune(self.h, cache_path.encode() if cache_path else None,
+                                           int(force), v))
+        return list(v)
 
     def measure_peaks(self) -> dict:
         v = [ctypes.c_double() for _ in range(4)]

@@ -49,7 +49,8 @@ class CBatch(ctypes.Structure):
 class Options(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("force_fp64", ctypes.c_int32),
                 ("device_memory_budget", ctypes.c_uint64), ("max_inflight", ctypes.c_uint32),
-                ("verbose", ctypes.c_int32)]
+                ("verbose", ctypes.c_int32), ("autotune", ctypes.c_int32),
+                ("tune_cache", ctypes.c_char_p)]
 
 
 class Stats(ctypes.Structure):
@@ -88,6 +89,8 @@ SIGNATURES = [
     ("rodv_measure_peaks", ctypes.c_int32, [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p]),
     ("rodv_pairhmm_batch_noalloc", ctypes.c_int32, [ctypes.POINTER(CBatch), ctypes.c_int32,
                                                     ctypes.c_void_p, ctypes.c_void_p]),
+    ("rodv_autotune", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int32,
+                                       ctypes.POINTER(ctypes.c_int32)]),
     ("rodv_status_string", ctypes.c_char_p, [ctypes.c_int32]),
     ("rodv_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
 ]

@@ -7,6 +7,8 @@
 
 using rodv::Engine;
 
+static_assert(RODV_TUNE_CLASSES == rodv::kNumClasses, "tuning classes out of sync");
+
 extern "C" {
 
 void rodv_default_options(rodv_options* opts) {
@@ -17,6 +19,8 @@ void rodv_default_options(rodv_options* opts) {
   opts->device_memory_budget = 0;
   opts->max_inflight = 0;
   opts->verbose = 0;
+  opts->autotune = 0;
+  opts->tune_cache = nullptr;
 }
 
 rodv_status rodv_engine_create(const rodv_options* opts, rodv_engine** out) {
@@ -135,6 +139,13 @@ rodv_status rodv_measure_peaks(rodv_engine* engine, double* f32, double* f32x2, 
   if (!engine) return RODV_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> lk(engine->impl->mutex());
   return engine->impl->measure_peaks(f32, f32x2, f64, mhz);
+}
+
+rodv_status rodv_autotune(rodv_engine* engine, const char* cache_path, int32_t force,
+                          int32_t* variants_out) {
+  if (!engine) return RODV_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(engine->impl->mutex());
+  return engine->impl->autotune(cache_path, force, variants_out);
 }
 
 const char* rodv_status_string(rodv_status s) {

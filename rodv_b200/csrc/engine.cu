@@ -1,27 +1,30 @@
 // engine.cu -- host side of the PairHMM engine: validation, packing, class
-// planning, persistent launches, FP64 rescue, results.
+// planning, persistent launches, FP64 rescue, autotuning, results.
 //
 // Control flow of one batch (the B200 counterpart of schedule_pairhmm,
 // src/core/pairhmm_schedule.cpp:116-340):
-//   1. validate and pack on the host (threads over reads) into one pinned
-//      staging buffer laid out exactly like the device arena;
+//   1. validate and pack on the host (threads over regions and reads) into one
+//      pinned staging buffer laid out exactly like the device arena;
 //   2. one H2D copy of the staging buffer;
-//   3. for each work class with pairs, one persistent FP32 launch over its
-//      items (two pairs per warp); pairs whose scaled FP32 result is below
-//      1e-28 are appended to the class's rescue list on the device;
-//   4. for each class, one persistent FP64 launch that drains the rescue list
-//      (its length is read by the kernel, never by the host);
+//   3. per work class, one persistent FP32 launch over its same-haplotype
+//      items (two reads of a region against one haplotype per warp) and one
+//      over the leftover two-haplotype items; pairs whose scaled FP32 result
+//      is below 1e-28 are appended to the class's FP64 list on the device;
+//   4. per work class, one persistent FP64 launch that drains that list (its
+//      length is read by the kernel, never by the host);
 //   5. one D2H copy of the log10 results.
 // The reference instead groups pairs into SIMD-width groups by padded area
-// (greedy_grouping, :46-105) and sends leftovers to a per-pair kernel; on the
-// GPU every pair goes through the same batched kernels, and work classes
-// (rows per lane) play the part of its idle-ratio grouping.
+// (greedy_grouping, :46-105) and sends leftovers to a per-pair kernel; here
+// work classes (rows per lane) and same-haplotype pairing play that part.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cstring>
+#include <fstream>
+#include <random>
+#include <sstream>
 #include <thread>
 
 #include "engine.h"
@@ -75,8 +78,7 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 // Device-arena views of a packed plan.
 struct ArenaView {
   BatchView view;
-  uint32_t* counts;   // [kNumClasses] fp32 counters, [kNumClasses] fp64 counters,
-                      // [kNumClasses] rescue counts, [1] error flags
+  uint32_t* counts;
   float* scratch;
 };
 
@@ -86,14 +88,21 @@ ArenaView arena_view(const PackedPlan& p, uint8_t* base, const PriorTables& tab)
   a.view.read_rows = reinterpret_cast<const uint32_t*>(base + p.off_read_rows);
   a.view.haps = reinterpret_cast<const HapDesc*>(base + p.off_haps);
   a.view.reads = reinterpret_cast<const ReadDesc*>(base + p.off_reads);
-  a.view.pairs = reinterpret_cast<const PairDesc*>(base + p.off_pairs);
   a.view.out = reinterpret_cast<double*>(base + p.off_out);
   a.view.tab = tab;
   a.counts = reinterpret_cast<uint32_t*>(base + p.off_counts);
   a.scratch = p.scratch_bytes ? reinterpret_cast<float*>(base + p.off_scratch) : nullptr;
   return a;
 }
-constexpr int kCountWords = 3 * kNumClasses + 1;
+
+// Occupancy variant used before (or without) tuning: the register budget
+// measured best for each rows-per-lane value on B200.
+int default_variant(int cls) {
+  const int R = class_rows(cls);
+  if (class_multi(cls) || R >= 7) return 0;  // 4 blocks/SM: up to 128 registers
+  if (R >= 4) return 2;                      // 6 blocks/SM: up to 80 registers
+  return 3;                                  // 8 blocks/SM: up to 64 registers
+}
 
 }  // namespace
 
@@ -122,7 +131,9 @@ cudaError_t PinnedMem::ensure(size_t n) {
   return e;
 }
 
-Engine::Engine(const rodv_options& opt) : opt_(opt) {}
+Engine::Engine(const rodv_options& opt) : opt_(opt) {
+  for (int c = 0; c < kNumClasses; ++c) variant_[c] = default_variant(c);
+}
 
 Engine::~Engine() {
   if (ready_) {
@@ -164,6 +175,7 @@ rodv_status Engine::init() {
     return fail(RODV_ERR_NO_DEVICE, std::string("engine is built for sm_100a; device is ") +
                                         prop.name);
   num_sms_ = prop.multiProcessorCount;
+  device_name_ = prop.name;
   RODV_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   for (auto& e : ev_) RODV_CUDA(cudaEventCreate(&e));
   const HostPriorTables& t = host_prior_tables();
@@ -183,6 +195,11 @@ rodv_status Engine::init() {
   tab_.mm_d = static_cast<const double*>(put(t.mm_d.data(), kMmTableSize * 8));
   RODV_CUDA(cudaGetLastError());
   ready_ = true;
+  if (opt_.tune_cache && opt_.tune_cache[0]) load_tuning(opt_.tune_cache);
+  if (opt_.autotune) {
+    rodv_status s = autotune(opt_.tune_cache, opt_.autotune > 1, nullptr);
+    if (s != RODV_OK) return s;
+  }
   return RODV_OK;
 }
 
@@ -205,9 +222,9 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   if (!b.hap_bases || !b.hap_offsets || !b.hap_lengths || !b.read_bases || !b.base_quals ||
       !b.ins_quals || !b.del_quals || !b.gcp_quals || !b.read_offsets || !b.read_lengths)
     return fail(RODV_ERR_INVALID_ARG, "null array in batch");
-  // regions
+  const uint32_t G = b.num_regions;
   uint64_t pairs = 0;
-  for (uint32_t g = 0; g < b.num_regions; ++g) {
+  for (uint32_t g = 0; g < G; ++g) {
     const rodv_region& r = b.regions[g];
     if (r.num_haps == 0 || r.num_reads == 0)
       return fail(RODV_ERR_EMPTY, "region " + std::to_string(g) + " has no haplotypes or reads");
@@ -220,8 +237,9 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   plan.num_pairs = pairs;
   plan.num_haps = b.num_haps;
   plan.num_reads = b.num_reads;
+  plan.regions.assign(b.regions, b.regions + G);
 
-  // haplotype code buffer: [pad][hap 0][pad][hap 1]...[hap n-1][pad + max len]
+  // haplotype code buffer: [pad][hap 0][pad][hap 1]...[hap n-1][pad + max len + pad]
   std::vector<uint64_t> hap_code_off(b.num_haps);
   uint64_t hb = 0;
   uint32_t max_h = 0;
@@ -249,20 +267,9 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   }
   plan.read_rows = rows;
 
-  // ---- arena layout ----
-  size_t o = 0;
-  plan.off_hap_codes = o; o = align_up(o + hb);
-  plan.off_read_rows = o; o = align_up(o + rows * 4);
-  plan.off_haps = o; o = align_up(o + (size_t)b.num_haps * sizeof(HapDesc));
-  plan.off_reads = o; o = align_up(o + (size_t)b.num_reads * sizeof(ReadDesc));
-  plan.off_pairs = o; o = align_up(o + pairs * sizeof(PairDesc));
-  // class counts need read flags first: compute them with the read pass below
-  // (item/list offsets are filled after counting).
-  const size_t fixed_end = o;
-
-  // ---- pass 1: read flags (uniform gaps) and class of every read ----
-  std::vector<uint8_t> read_uniform(b.num_reads);
-  std::atomic<int> bad_base{-1};
+  // ---- read flags (uniform gaps) and class of every read ----
+  std::vector<uint8_t>& read_class = plan.read_class;
+  read_class.resize(b.num_reads);
   parallel_for(b.num_reads, 4096, [&](size_t lo, size_t hi) {
     for (size_t r = lo; r < hi; ++r) {
       const uint64_t off = b.read_offsets[r];
@@ -275,63 +282,101 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
             (b.gcp_quals[off + k] & 127) == c0;
       // The uniform-gap kernels store M/gapm; gcp quality 0 gives gapm = 0,
       // so such reads take the per-row kernels.
-      read_uniform[r] = (u && c0 != 0) ? 1 : 0;
+      read_class[r] = (uint8_t)class_of(n, u && c0 != 0);
     }
   });
-  std::vector<uint8_t> read_class(b.num_reads);
-  for (uint32_t r = 0; r < b.num_reads; ++r)
-    read_class[r] = (uint8_t)class_of(b.read_lengths[r], read_uniform[r] != 0);
 
-  // ---- per-class pair counts and the largest haplotype of multi-pass pairs ----
-  for (uint32_t g = 0; g < b.num_regions; ++g) {
+  // ---- per region and class: reads, same items, leftovers, pairs ----
+  std::vector<uint32_t> rc((size_t)G * kNumClasses, 0);   // reads of class c in region g
+  parallel_for(G, 256, [&](size_t lo, size_t hi) {
+    for (size_t g = lo; g < hi; ++g) {
+      const rodv_region& rg = b.regions[g];
+      for (uint32_t r = 0; r < rg.num_reads; ++r) rc[g * kNumClasses + read_class[rg.read_start + r]]++;
+    }
+  });
+  // prefix offsets (within each class) of same items, leftovers, FP64 list entries
+  std::vector<uint64_t> same_off((size_t)G * kNumClasses), left_off((size_t)G * kNumClasses),
+      list_off((size_t)G * kNumClasses);
+  uint64_t same_tot[kNumClasses] = {}, left_tot[kNumClasses] = {}, list_tot[kNumClasses] = {};
+  for (uint32_t g = 0; g < G; ++g) {
+    const uint64_t H = b.regions[g].num_haps;
+    for (int c = 0; c < kNumClasses; ++c) {
+      const uint64_t n = rc[(size_t)g * kNumClasses + c];
+      same_off[(size_t)g * kNumClasses + c] = same_tot[c];
+      left_off[(size_t)g * kNumClasses + c] = left_tot[c];
+      list_off[(size_t)g * kNumClasses + c] = list_tot[c];
+      same_tot[c] += H * (n / 2);
+      left_tot[c] += H * (n & 1);
+      list_tot[c] += H * n;
+    }
+  }
+  for (int c = 0; c < kNumClasses; ++c) {
+    plan.pairs[c] = (uint32_t)list_tot[c];
+    plan.same_items[c] = fp64 ? 0u : (uint32_t)same_tot[c];
+    plan.diff_items[c] = fp64 ? 0u : (uint32_t)((left_tot[c] + 1) / 2);
+  }
+  for (uint32_t g = 0; g < G; ++g) {
     const rodv_region& rg = b.regions[g];
-    uint32_t rc[kNumClasses] = {};
-    for (uint32_t r = 0; r < rg.num_reads; ++r) rc[read_class[rg.read_start + r]]++;
-    for (int c = 0; c < kNumClasses; ++c) plan.pairs[c] += rc[c] * rg.num_haps;
-    if (rc[kSinglePassClasses] || rc[kSinglePassClasses + 1])
+    if (rc[(size_t)g * kNumClasses + kSinglePassClasses] ||
+        rc[(size_t)g * kNumClasses + kSinglePassClasses + 1])
       for (uint32_t h = 0; h < rg.num_haps; ++h)
         plan.multi_max_hap = std::max(plan.multi_max_hap, b.hap_lengths[rg.hap_start + h]);
   }
-  o = fixed_end;
+
+  // ---- arena layout ----
+  size_t o = 0;
+  plan.off_hap_codes = o; o = align_up(o + hb);
+  plan.off_read_rows = o; o = align_up(o + rows * 4);
+  plan.off_haps = o; o = align_up(o + (size_t)b.num_haps * sizeof(HapDesc));
+  plan.off_reads = o; o = align_up(o + (size_t)b.num_reads * sizeof(ReadDesc));
   for (int c = 0; c < kNumClasses; ++c) {
-    plan.items[c] = fp64 ? 0 : (plan.pairs[c] + 1) / 2;
-    plan.off_items[c] = o;
-    o = align_up(o + (size_t)plan.items[c] * sizeof(Item));
-    plan.off_lists[c] = o;
-    o = align_up(o + (size_t)plan.pairs[c] * 4);
+    plan.off_same[c] = o;
+    o = align_up(o + (size_t)plan.same_items[c] * sizeof(SameItem));
   }
-  plan.upload_bytes = o;
+  for (int c = 0; c < kNumClasses; ++c) {
+    plan.off_diff[c] = o;
+    o = align_up(o + (size_t)plan.diff_items[c] * sizeof(DiffItem));
+  }
+  const size_t lists_begin = o;
+  for (int c = 0; c < kNumClasses; ++c) {
+    plan.off_lists[c] = o;
+    o = align_up(o + (size_t)plan.pairs[c] * sizeof(PairRef));
+  }
+  // FP32 runs fill the lists on the device; only forced-FP64 lists are uploaded.
+  plan.upload_bytes = fp64 ? o : lists_begin;
   plan.off_out = o; o = align_up(o + pairs * 8);
   plan.off_counts = o; o = align_up(o + kCountWords * 4);
   plan.scratch_cols = plan.multi_max_hap ? plan.multi_max_hap + 40 : 0;
   plan.off_scratch = o;
   if (plan.scratch_cols) {
-    int blocks = 0, warps = 0;
+    int warps = 0;
     for (int u = 0; u < 2; ++u)
-      for (int p = 0; p < 2; ++p) {
-        const KernelInfo k = forward_kernel_info(p ? Precision::kF64 : Precision::kF32x2,
-                                                 kMaxRowsPerLane, u != 0, true);
-        blocks = persistent_blocks(k);
-        warps = std::max(warps, blocks * k.warps_per_block);
-      }
+      for (int p = 0; p < 3; ++p)
+        for (int v = 0; v < kTuneVariants; ++v) {
+          const Precision pr = p == 2 ? Precision::kF64 : Precision::kF32x2;
+          if (v > 0 && forward_kernel_variants(pr, p == 0) == 1) continue;
+          const KernelInfo k = forward_kernel_info(pr, kMaxRowsPerLane, u != 0, true, p == 0, v);
+          warps = std::max(warps, persistent_blocks(k) * k.warps_per_block);
+        }
     plan.scratch_bytes = (size_t)warps * plan.scratch_cols * 24;
     o = align_up(o + plan.scratch_bytes);
   }
   plan.total_bytes = o;
 
-  cudaError_t e = staging.ensure(plan.upload_bytes);
+  cudaError_t e = staging.ensure(std::max<size_t>(plan.upload_bytes, 1));
   if (e != cudaSuccess) return cuda_fail(e, "pinned staging allocation");
   uint8_t* s = static_cast<uint8_t*>(staging.ptr);
 
   // ---- haplotype codes ----
+  std::atomic<int> bad_base{-1};
   uint8_t* codes = s + plan.off_hap_codes;
-  std::memset(codes, 0, hb);
   HapDesc* hd = reinterpret_cast<HapDesc*>(s + plan.off_haps);
   parallel_for(b.num_haps, 256, [&](size_t lo, size_t hi) {
     for (size_t h = lo; h < hi; ++h) {
       const uint8_t* src = b.hap_bases + b.hap_offsets[h];
       uint8_t* dst = codes + hap_code_off[h];
       const uint32_t n = b.hap_lengths[h];
+      std::memset(dst - kHapPad, 0, kHapPad);
       for (uint32_t k = 0; k < n; ++k) {
         const uint8_t c = kCodes.v[src[k]];
         if (c == 0xff) bad_base.store((int)src[k]);
@@ -342,6 +387,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       hd[h].pad_ = 0;
     }
   });
+  std::memset(codes + hb - (kHapPad + max_h + kHapPad), 0, kHapPad + max_h + kHapPad);
   // ---- read rows ----
   uint32_t* rw = reinterpret_cast<uint32_t*>(s + plan.off_read_rows);
   ReadDesc* rdesc = reinterpret_cast<ReadDesc*>(s + plan.off_reads);
@@ -359,7 +405,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       for (uint32_t k = n; k < ((n + 3) & ~3u); ++k) dst[k] = 0;
       rdesc[r].row_off = row_off[r];
       rdesc[r].len = n;
-      rdesc[r].flags = read_uniform[r] ? kReadUniformGaps : 0u;
+      rdesc[r].flags = (read_class[r] & 1) ? kReadUniformGaps : 0u;
     }
   });
   if (bad_base.load() >= 0) {
@@ -368,73 +414,61 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
     return fail(RODV_ERR_INVALID_BASE, msg);
   }
 
-  // ---- pairs (result order) and per-class lists sorted by haplotype length ----
-  PairDesc* pd = reinterpret_cast<PairDesc*>(s + plan.off_pairs);
-  std::vector<uint64_t> region_off(b.num_regions + 1, 0);
-  for (uint32_t g = 0; g < b.num_regions; ++g)
-    region_off[g + 1] = region_off[g] + (uint64_t)b.regions[g].num_haps * b.regions[g].num_reads;
-  parallel_for(b.num_regions, 64, [&](size_t lo, size_t hi) {
+  // ---- work: same-haplotype items, leftovers, forced-FP64 lists ----
+  std::vector<uint64_t> region_out(G);
+  for (uint32_t g = 0, acc = 0; g < G; ++g) {
+    region_out[g] = acc;
+    acc += b.regions[g].num_haps * b.regions[g].num_reads;
+  }
+  std::vector<PairRef> leftovers[kNumClasses];
+  for (int c = 0; c < kNumClasses; ++c) leftovers[c].resize(left_tot[c]);
+  parallel_for(G, 64, [&](size_t lo, size_t hi) {
+    std::vector<uint32_t> byclass[kNumClasses];
     for (size_t g = lo; g < hi; ++g) {
       const rodv_region& rg = b.regions[g];
-      uint64_t p = region_off[g];
-      for (uint32_t h = 0; h < rg.num_haps; ++h)
-        for (uint32_t r = 0; r < rg.num_reads; ++r, ++p) {
-          pd[p].hap = rg.hap_start + h;
-          pd[p].read = rg.read_start + r;
-          pd[p].out = p;
-        }
-    }
-  });
-  // counting sort by (class, hap length descending)
-  const uint32_t nbins = max_h + 1;
-  std::vector<uint32_t> hist((size_t)kNumClasses * nbins, 0);
-  for (uint32_t g = 0; g < b.num_regions; ++g) {
-    const rodv_region& rg = b.regions[g];
-    uint32_t rc[kNumClasses] = {};
-    for (uint32_t r = 0; r < rg.num_reads; ++r) rc[read_class[rg.read_start + r]]++;
-    for (uint32_t h = 0; h < rg.num_haps; ++h) {
-      const uint32_t hl = b.hap_lengths[rg.hap_start + h];
-      for (int c = 0; c < kNumClasses; ++c) hist[(size_t)c * nbins + (max_h - hl)] += rc[c];
-    }
-  }
-  // exclusive prefix per class
-  for (int c = 0; c < kNumClasses; ++c) {
-    uint32_t acc = 0;
-    for (uint32_t k = 0; k < nbins; ++k) {
-      const uint32_t v = hist[(size_t)c * nbins + k];
-      hist[(size_t)c * nbins + k] = acc;
-      acc += v;
-    }
-  }
-  {
-    uint64_t p = 0;
-    for (uint32_t g = 0; g < b.num_regions; ++g) {
-      const rodv_region& rg = b.regions[g];
-      for (uint32_t h = 0; h < rg.num_haps; ++h) {
-        const uint32_t hl = b.hap_lengths[rg.hap_start + h];
-        for (uint32_t r = 0; r < rg.num_reads; ++r, ++p) {
-          const int c = read_class[rg.read_start + r];
-          uint32_t* list = reinterpret_cast<uint32_t*>(s + plan.off_lists[c]);
-          list[hist[(size_t)c * nbins + (max_h - hl)]++] = (uint32_t)p;
+      for (auto& v : byclass) v.clear();
+      for (uint32_t r = 0; r < rg.num_reads; ++r)
+        byclass[read_class[rg.read_start + r]].push_back(rg.read_start + r);
+      for (int c = 0; c < kNumClasses; ++c) {
+        const std::vector<uint32_t>& rd = byclass[c];
+        if (rd.empty()) continue;
+        SameItem* si = reinterpret_cast<SameItem*>(s + plan.off_same[c]) +
+                       same_off[g * kNumClasses + c];
+        PairRef* lf = leftovers[c].data() + left_off[g * kNumClasses + c];
+        PairRef* li = reinterpret_cast<PairRef*>(s + plan.off_lists[c]) +
+                      list_off[g * kNumClasses + c];
+        for (uint32_t h = 0; h < rg.num_haps; ++h) {
+          const uint32_t hap = rg.hap_start + h;
+          const uint64_t base = region_out[g] + (uint64_t)h * rg.num_reads - rg.read_start;
+          if (fp64) {
+            for (uint32_t rr : rd) *li++ = PairRef{hap, rr, (uint32_t)(base + rr)};
+            continue;
+          }
+          size_t k = 0;
+          for (; k + 1 < rd.size(); k += 2)
+            *si++ = SameItem{hap, rd[k], rd[k + 1], (uint32_t)(base + rd[k])};
+          if (k < rd.size()) *lf++ = PairRef{hap, rd[k], (uint32_t)(base + rd[k])};
         }
       }
     }
-  }
-  // FP32 items: consecutive pairs of the sorted list (longer haplotype first)
+  });
   if (!fp64) {
+    // leftovers: sorted by haplotype length, paired longest-first
     for (int c = 0; c < kNumClasses; ++c) {
-      const uint32_t* list = reinterpret_cast<const uint32_t*>(s + plan.off_lists[c]);
-      Item* it = reinterpret_cast<Item*>(s + plan.off_items[c]);
-      const uint32_t n = plan.pairs[c];
-      for (uint32_t k = 0; k < plan.items[c]; ++k) {
-        it[k].x = list[2 * k];
-        it[k].y = (2 * k + 1 < n) ? list[2 * k + 1] : kNoPair;
+      std::vector<PairRef>& lv = leftovers[c];
+      std::stable_sort(lv.begin(), lv.end(), [&](const PairRef& x, const PairRef& y) {
+        return b.hap_lengths[x.hap] > b.hap_lengths[y.hap];
+      });
+      DiffItem* di = reinterpret_cast<DiffItem*>(s + plan.off_diff[c]);
+      for (size_t k = 0; k < plan.diff_items[c]; ++k) {
+        di[k].x = lv[2 * k];
+        di[k].y = (2 * k + 1 < lv.size()) ? lv[2 * k + 1] : PairRef{0, kNoPair, 0};
       }
     }
   }
   // cells
   uint64_t cells = 0;
-  for (uint32_t g = 0; g < b.num_regions; ++g) {
+  for (uint32_t g = 0; g < G; ++g) {
     const rodv_region& rg = b.regions[g];
     uint64_t hs = 0, rs = 0;
     for (uint32_t h = 0; h < rg.num_haps; ++h) hs += b.hap_lengths[rg.hap_start + h];
@@ -448,45 +482,52 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
 // ---------------------------------------------------------------------------
 // Launches
 // ---------------------------------------------------------------------------
+rodv_status Engine::launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, int c, bool same,
+                                      int variant, int blocks_cap) {
+  ArenaView a = arena_view(plan, dbase, tab_);
+  const uint32_t n = same ? plan.same_items[c] : plan.diff_items[c];
+  if (!n) return RODV_OK;
+  const KernelInfo k = forward_kernel_info(Precision::kF32x2, class_rows(c), class_uniform(c),
+                                           class_multi(c), same, same ? variant : 0);
+  ClassLaunch cl{};
+  cl.work = dbase + (same ? plan.off_same[c] : plan.off_diff[c]);
+  cl.work_count = nullptr;
+  cl.static_count = n;
+  cl.counter = a.counts + (same ? kCtrSame : kCtrDiff) + c;
+  cl.rescue_list = reinterpret_cast<PairRef*>(dbase + plan.off_lists[c]);
+  cl.rescue_count = a.counts + kCtrRescue + c;
+  cl.scratch = a.scratch;
+  cl.scratch_cols = plan.scratch_cols;
+  cl.error_flags = a.counts + kCtrError;
+  const int need = (int)((n + k.warps_per_block - 1) / k.warps_per_block);
+  int blocks = std::max(1, std::min(persistent_blocks(k), need));
+  if (blocks_cap > 0) blocks = std::min(blocks, blocks_cap);
+  void* args[] = {&a.view, &cl};
+  RODV_CUDA(cudaLaunchKernel(k.fn, dim3(blocks), dim3(k.threads), args, k.smem_bytes, stream_));
+  return RODV_OK;
+}
+
 rodv_status Engine::launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stats* st,
                                bool timed) {
   ArenaView a = arena_view(plan, dbase, tab_);
-  uint32_t* fp32_ctr = a.counts;
-  uint32_t* fp64_ctr = a.counts + kNumClasses;
-  uint32_t* rescue_cnt = a.counts + 2 * kNumClasses;
-  uint32_t* err = a.counts + 3 * kNumClasses;
-  const bool fp64 = plan.fp64;
   RODV_CUDA(cudaMemsetAsync(a.counts, 0, kCountWords * 4, stream_));
-  if (fp64) {
-    // every pair goes to the FP64 kernels: the lists are the class lists
+  if (plan.fp64) {
+    // every pair goes to the FP64 kernels: the uploaded lists are full
     std::vector<uint32_t> preset(kNumClasses);
     for (int c = 0; c < kNumClasses; ++c) preset[c] = plan.pairs[c];
-    RODV_CUDA(cudaMemcpyAsync(rescue_cnt, preset.data(), kNumClasses * 4, cudaMemcpyHostToDevice,
-                              stream_));
+    RODV_CUDA(cudaMemcpyAsync(a.counts + kCtrRescue, preset.data(), kNumClasses * 4,
+                              cudaMemcpyHostToDevice, stream_));
   }
   uint32_t launches = 0;
   if (timed) RODV_CUDA(cudaEventRecord(ev_[0], stream_));
-  if (!fp64) {
+  if (!plan.fp64) {
     for (int c = 0; c < kNumClasses; ++c) {
-      if (!plan.items[c]) continue;
-      const KernelInfo k = forward_kernel_info(Precision::kF32x2, class_rows(c), class_uniform(c),
-                                               class_multi(c));
-      ClassLaunch cl{};
-      cl.work = reinterpret_cast<const uint32_t*>(dbase + plan.off_items[c]);
-      cl.work_count = nullptr;
-      cl.static_count = plan.items[c];
-      cl.counter = fp32_ctr + c;
-      cl.rescue_list = reinterpret_cast<uint32_t*>(dbase + plan.off_lists[c]);
-      cl.rescue_count = rescue_cnt + c;
-      cl.scratch = a.scratch;
-      cl.scratch_cols = plan.scratch_cols;
-      cl.error_flags = err;
-      const int need = (int)((plan.items[c] + k.warps_per_block - 1) / k.warps_per_block);
-      const int blocks = std::max(1, std::min(persistent_blocks(k), need));
-      void* args[] = {&a.view, &cl};
-      RODV_CUDA(cudaLaunchKernel(k.fn, dim3(blocks), dim3(k.threads), args, k.smem_bytes,
-                                 stream_));
-      ++launches;
+      for (int same = 1; same >= 0; --same) {
+        if (!(same ? plan.same_items[c] : plan.diff_items[c])) continue;
+        rodv_status s = launch_fp32_class(plan, dbase, c, same != 0, variant_[c], 0);
+        if (s != RODV_OK) return s;
+        ++launches;
+      }
     }
   }
   if (timed) RODV_CUDA(cudaEventRecord(ev_[1], stream_));
@@ -495,15 +536,13 @@ rodv_status Engine::launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stat
     const KernelInfo k =
         forward_kernel_info(Precision::kF64, class_rows(c), class_uniform(c), class_multi(c));
     ClassLaunch cl{};
-    cl.work = reinterpret_cast<const uint32_t*>(dbase + plan.off_lists[c]);
-    cl.work_count = rescue_cnt + c;
+    cl.work = dbase + plan.off_lists[c];
+    cl.work_count = a.counts + kCtrRescue + c;
     cl.static_count = 0;
-    cl.counter = fp64_ctr + c;
-    cl.rescue_list = nullptr;
-    cl.rescue_count = nullptr;
+    cl.counter = a.counts + kCtrF64 + c;
     cl.scratch = a.scratch;
     cl.scratch_cols = plan.scratch_cols;
-    cl.error_flags = err;
+    cl.error_flags = a.counts + kCtrError;
     const int need = (int)((plan.pairs[c] + k.warps_per_block - 1) / k.warps_per_block);
     const int blocks = std::max(1, std::min(persistent_blocks(k), need));
     void* args[] = {&a.view, &cl};
@@ -516,22 +555,19 @@ rodv_status Engine::launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stat
 }
 
 rodv_status Engine::check_errors(const PackedPlan& plan, uint8_t* dbase) {
-  uint32_t tail[kNumClasses + 1];
-  RODV_CUDA(cudaMemcpy(tail, dbase + plan.off_counts + 2 * kNumClasses * 4,
-                       sizeof(tail), cudaMemcpyDeviceToHost));
-  if (tail[kNumClasses] != 0)
-    return fail(RODV_ERR_DEVICE_CHECK,
-                "kernel reported error flags " + std::to_string(tail[kNumClasses]));
+  uint32_t err = 0;
+  RODV_CUDA(cudaMemcpy(&err, dbase + plan.off_counts + kCtrError * 4, 4, cudaMemcpyDeviceToHost));
+  if (err != 0)
+    return fail(RODV_ERR_DEVICE_CHECK, "kernel reported error flags " + std::to_string(err));
   return RODV_OK;
 }
 
-static void fill_stats(rodv_stats* st, const PackedPlan& plan, const uint32_t* rescue,
-                       bool fp64) {
+static void fill_stats(rodv_stats* st, const PackedPlan& plan, const uint32_t* counts) {
   if (!st) return;
   st->pairs = plan.num_pairs;
   st->cells = plan.cells;
   uint64_t n = 0;
-  for (int c = 0; c < kNumClasses; ++c) n += fp64 ? plan.pairs[c] : rescue[c];
+  for (int c = 0; c < kNumClasses; ++c) n += plan.fp64 ? plan.pairs[c] : counts[kCtrRescue + c];
   st->fp64_pairs = n;
 }
 
@@ -556,12 +592,12 @@ rodv_status Engine::run_host(const rodv_batch& b, double* out, rodv_stats* st, b
                             cudaMemcpyDeviceToHost, stream_));
   RODV_CUDA(cudaStreamSynchronize(stream_));
   const uint32_t* counts = reinterpret_cast<const uint32_t*>(hs + plan.num_pairs * 8);
-  if (counts[3 * kNumClasses] != 0)
+  if (counts[kCtrError] != 0)
     return fail(RODV_ERR_DEVICE_CHECK,
-                "kernel reported error flags " + std::to_string(counts[3 * kNumClasses]));
+                "kernel reported error flags " + std::to_string(counts[kCtrError]));
   std::memcpy(out, hs, plan.num_pairs * 8);
   if (st) {
-    fill_stats(st, plan, counts + 2 * kNumClasses, plan.fp64);
+    fill_stats(st, plan, counts);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ev_[0], ev_[2]);
     st->device_ms = ms;
@@ -605,11 +641,10 @@ rodv_status Engine::run_device(rodv_device_batch* db, rodv_stats* st) {
   rodv_status s = launch_all(db->plan, d, st, true);
   if (s != RODV_OK) return s;
   RODV_CUDA(cudaStreamSynchronize(stream_));
+  uint32_t counts[kCountWords];
+  RODV_CUDA(cudaMemcpy(counts, d + db->plan.off_counts, sizeof(counts), cudaMemcpyDeviceToHost));
   if (st) {
-    uint32_t counts[kCountWords];
-    RODV_CUDA(cudaMemcpy(counts, d + db->plan.off_counts, sizeof(counts),
-                         cudaMemcpyDeviceToHost));
-    fill_stats(st, db->plan, counts + 2 * kNumClasses, db->plan.fp64);
+    fill_stats(st, db->plan, counts);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ev_[0], ev_[2]);
     st->device_ms = ms;
@@ -617,7 +652,10 @@ rodv_status Engine::run_device(rodv_device_batch* db, rodv_stats* st) {
     st->fp32_ms = ms;
     st->total_ms = ms_since(t0);
   }
-  return check_errors(db->plan, d);
+  if (counts[kCtrError] != 0)
+    return fail(RODV_ERR_DEVICE_CHECK,
+                "kernel reported error flags " + std::to_string(counts[kCtrError]));
+  return RODV_OK;
 }
 
 rodv_status Engine::download(rodv_device_batch* db, double* out) {
@@ -627,7 +665,7 @@ rodv_status Engine::download(rodv_device_batch* db, double* out) {
   return RODV_OK;
 }
 
-// The plain GPU form: every pair is its own FP32 launch (one warp, slot y
+// The plain GPU form: every pair is its own FP32 launch (one warp, second slot
 // empty), its result is read back, and a pair below 1e-28 gets a second,
 // FP64 launch.  Same kernels as the batched path; no batching.
 rodv_status Engine::plain(rodv_device_batch* db, double* out, rodv_stats* st) {
@@ -635,55 +673,59 @@ rodv_status Engine::plain(rodv_device_batch* db, double* out, rodv_stats* st) {
   const PackedPlan& plan = db->plan;
   uint8_t* d = static_cast<uint8_t*>(db->arena.ptr);
   ArenaView a = arena_view(plan, d, tab_);
-  // scratch words: [0..1] item, [2] pair id, [3] fp32 counter, [4] fp64 counter,
-  // [5] rescue count, [6] rescue list entry, [7] error flags
+  // control block: [0,16) SameItem, [16,28) rescue PairRef, words 8..11:
+  // fp32 counter, fp64 counter, rescue count, error flags
   DeviceMem ctl;
   RODV_CUDA(ctl.ensure(64));
-  uint32_t* w = static_cast<uint32_t*>(ctl.ptr);
+  uint8_t* w = static_cast<uint8_t*>(ctl.ptr);
+  uint32_t* wc = reinterpret_cast<uint32_t*>(w + 32);
   PinnedMem host;
   RODV_CUDA(host.ensure(64));
-  uint32_t* hw = static_cast<uint32_t*>(host.ptr);
-  std::vector<PairDesc> pairs(plan.num_pairs);
-  std::vector<ReadDesc> reads(plan.num_reads);
-  RODV_CUDA(cudaMemcpy(pairs.data(), d + plan.off_pairs, plan.num_pairs * sizeof(PairDesc),
-                       cudaMemcpyDeviceToHost));
-  RODV_CUDA(cudaMemcpy(reads.data(), d + plan.off_reads, plan.num_reads * sizeof(ReadDesc),
-                       cudaMemcpyDeviceToHost));
+  uint8_t* hw = static_cast<uint8_t*>(host.ptr);
+  uint32_t* hc = reinterpret_cast<uint32_t*>(hw + 32);
   uint32_t launches = 0;
   uint64_t rescued = 0;
   const auto t0 = std::chrono::steady_clock::now();
   RODV_CUDA(cudaEventRecord(ev_[0], stream_));
-  for (uint64_t p = 0; p < plan.num_pairs; ++p) {
-    const ReadDesc& rd = reads[pairs[p].read];
-    const int c = class_of(rd.len, (rd.flags & kReadUniformGaps) != 0);
-    hw[0] = (uint32_t)p;
-    hw[1] = kNoPair;
-    hw[2] = (uint32_t)p;
-    hw[3] = hw[4] = hw[5] = hw[6] = hw[7] = 0;
-    RODV_CUDA(cudaMemcpyAsync(w, hw, 32, cudaMemcpyHostToDevice, stream_));
-    for (int pass = 0; pass < 2; ++pass) {
-      const bool f64 = pass == 1 || plan.fp64;
-      const KernelInfo k = forward_kernel_info(f64 ? Precision::kF64 : Precision::kF32x2,
-                                               class_rows(c), class_uniform(c), class_multi(c));
-      ClassLaunch cl{};
-      cl.work = f64 ? w + 2 : w;
-      cl.work_count = nullptr;
-      cl.static_count = 1;
-      cl.counter = f64 ? w + 4 : w + 3;
-      cl.rescue_list = w + 6;
-      cl.rescue_count = w + 5;
-      cl.scratch = a.scratch;
-      cl.scratch_cols = plan.scratch_cols;
-      cl.error_flags = w + 7;
-      void* args[] = {&a.view, &cl};
-      RODV_CUDA(cudaLaunchKernel(k.fn, dim3(1), dim3(k.threads), args, k.smem_bytes, stream_));
-      ++launches;
-      if (f64) break;
-      RODV_CUDA(cudaMemcpyAsync(hw + 5, w + 5, 12, cudaMemcpyDeviceToHost, stream_));
-      RODV_CUDA(cudaStreamSynchronize(stream_));
-      if (hw[7]) return fail(RODV_ERR_DEVICE_CHECK, "plain kernel reported an error");
-      if (hw[5] == 0) break;
-      ++rescued;
+  uint64_t p = 0;
+  for (const rodv_region& rg : plan.regions) {
+    for (uint32_t h = 0; h < rg.num_haps; ++h) {
+      for (uint32_t r = 0; r < rg.num_reads; ++r, ++p) {
+        const uint32_t read = rg.read_start + r;
+        const int c = plan.read_class[read];
+        const SameItem item{rg.hap_start + h, read, kNoPair, (uint32_t)p};
+        std::memcpy(hw, &item, sizeof(item));
+        const PairRef ref{rg.hap_start + h, read, (uint32_t)p};
+        std::memcpy(hw + 16, &ref, sizeof(ref));
+        hc[0] = hc[1] = hc[2] = hc[3] = 0;
+        RODV_CUDA(cudaMemcpyAsync(w, hw, 48, cudaMemcpyHostToDevice, stream_));
+        for (int pass = 0; pass < 2; ++pass) {
+          const bool f64 = pass == 1 || plan.fp64;
+          const KernelInfo k =
+              forward_kernel_info(f64 ? Precision::kF64 : Precision::kF32x2, class_rows(c),
+                                  class_uniform(c), class_multi(c), true, variant_[c]);
+          ClassLaunch cl{};
+          cl.work = f64 ? static_cast<const void*>(w + 16) : static_cast<const void*>(w);
+          cl.work_count = nullptr;
+          cl.static_count = 1;
+          cl.counter = f64 ? wc + 1 : wc;
+          cl.rescue_list = reinterpret_cast<PairRef*>(w + 16);
+          cl.rescue_count = wc + 2;
+          cl.scratch = a.scratch;
+          cl.scratch_cols = plan.scratch_cols;
+          cl.error_flags = wc + 3;
+          void* args[] = {&a.view, &cl};
+          RODV_CUDA(
+              cudaLaunchKernel(k.fn, dim3(1), dim3(k.threads), args, k.smem_bytes, stream_));
+          ++launches;
+          if (f64) break;
+          RODV_CUDA(cudaMemcpyAsync(hc + 2, wc + 2, 8, cudaMemcpyDeviceToHost, stream_));
+          RODV_CUDA(cudaStreamSynchronize(stream_));
+          if (hc[3]) return fail(RODV_ERR_DEVICE_CHECK, "plain kernel reported an error");
+          if (hc[2] == 0) break;
+          ++rescued;
+        }
+      }
     }
   }
   RODV_CUDA(cudaEventRecord(ev_[1], stream_));
@@ -699,6 +741,137 @@ rodv_status Engine::plain(rodv_device_batch* db, double* out, rodv_stats* st) {
     st->total_ms = ms_since(t0);
   }
   if (out) return download(db, out);
+  return RODV_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuning: per work class, the occupancy variant (register budget) of the
+// same-haplotype FP32 kernel, chosen by timing every variant on a synthetic
+// batch of that class (reads of 32R-5 bases, or 700 for multi-pass, against
+// 400- or 1,200-base haplotypes).  Results are cached per device.
+// ---------------------------------------------------------------------------
+std::string Engine::device_key() const {
+  std::string k = device_name_;
+  for (char& ch : k)
+    if (ch == ' ') ch = '_';
+  return k + "_sm" + std::to_string(num_sms_);
+}
+
+bool Engine::load_tuning(const std::string& path) {
+  std::ifstream in(path);
+  if (!in) return false;
+  std::string line, key = device_key();
+  int found = 0;
+  while (std::getline(in, line)) {
+    std::istringstream ss(line);
+    std::string k;
+    int c, v;
+    if (!(ss >> k >> c >> v) || k != key) continue;
+    if (c >= 0 && c < kNumClasses && v >= 0 && v < kTuneVariants) {
+      variant_[c] = v;
+      ++found;
+    }
+  }
+  tuned_ = found == kNumClasses;
+  return tuned_;
+}
+
+bool Engine::save_tuning(const std::string& path) const {
+  std::ofstream out(path, std::ios::trunc);
+  if (!out) return false;
+  for (int c = 0; c < kNumClasses; ++c) out << device_key() << ' ' << c << ' ' << variant_[c] << '\n';
+  return (bool)out;
+}
+
+rodv_status Engine::autotune(const char* cache_path, int force, int32_t* variants_out) {
+  const std::string path = cache_path ? cache_path : "";
+  if (!force && !path.empty() && load_tuning(path)) {
+    if (variants_out)
+      for (int c = 0; c < kNumClasses; ++c) variants_out[c] = variant_[c];
+    return RODV_OK;
+  }
+  RODV_CUDA(cudaSetDevice(device_));
+  std::mt19937 rng(12345);
+  const char* acgt = "ACGT";
+  for (int c = 0; c < kNumClasses; ++c) {
+    const int R = class_rows(c);
+    const bool multi = class_multi(c), uni = class_uniform(c);
+    const uint32_t L = multi ? 700 : (uint32_t)std::max(1, 32 * R - 5);
+    const uint32_t H = multi ? 1200 : 400;
+    const int regions = 16, haps = 4;
+    const int reads = (int)std::max<uint64_t>(2, std::min<uint64_t>(512, 1500000000ull /
+                                                                        ((uint64_t)regions * haps * L * H)));
+    std::vector<uint8_t> hb, rb, q, ins, del, gcp;
+    std::vector<uint64_t> ho, ro;
+    std::vector<uint32_t> hl, rl;
+    std::vector<rodv_region> rg;
+    for (int g = 0; g < regions; ++g) {
+      rodv_region r{(uint32_t)ho.size(), (uint32_t)haps, (uint32_t)ro.size(), (uint32_t)reads};
+      std::string base;
+      for (uint32_t j = 0; j < H; ++j) base += acgt[rng() % 4];
+      for (int h = 0; h < haps; ++h) {
+        ho.push_back(hb.size());
+        hl.push_back(H);
+        for (uint32_t j = 0; j < H; ++j) hb.push_back(rng() % 100 ? base[j] : acgt[rng() % 4]);
+      }
+      for (int k = 0; k < reads; ++k) {
+        ro.push_back(rb.size());
+        rl.push_back(L);
+        const uint32_t st = rng() % (H - std::min(L, H) + 1);
+        for (uint32_t j = 0; j < L; ++j) {
+          rb.push_back(j + st < H && rng() % 100 ? base[j + st] : acgt[rng() % 4]);
+          q.push_back(10 + rng() % 31);
+          ins.push_back(uni ? 45 : 20 + rng() % 26);
+          del.push_back(uni ? 45 : 20 + rng() % 26);
+          gcp.push_back(uni ? 10 : 5 + rng() % 11);
+        }
+      }
+      rg.push_back(r);
+    }
+    rodv_batch b{(uint32_t)rg.size(), rg.data(), (uint32_t)hl.size(), hb.data(), ho.data(),
+                 hl.data(), (uint32_t)rl.size(), rb.data(), q.data(), ins.data(), del.data(),
+                 gcp.data(), ro.data(), rl.data()};
+    rodv_device_batch* db = nullptr;
+    rodv_status s = upload(b, &db);
+    if (s != RODV_OK) return s;
+    uint8_t* d = static_cast<uint8_t*>(db->arena.ptr);
+    const uint32_t* counts = reinterpret_cast<const uint32_t*>(d + db->plan.off_counts);
+    float best_ms = 1e30f;
+    int best_v = variant_[c];
+    for (int v = 0; v < kTuneVariants; ++v) {
+      float vbest = 1e30f;
+      for (int rep = 0; rep < 3; ++rep) {
+        RODV_CUDA(cudaMemsetAsync((void*)counts, 0, kCountWords * 4, stream_));
+        RODV_CUDA(cudaEventRecord(ev_[0], stream_));
+        s = launch_fp32_class(db->plan, d, c, true, v, 0);
+        if (s != RODV_OK) {
+          delete db;
+          return s;
+        }
+        RODV_CUDA(cudaEventRecord(ev_[1], stream_));
+        RODV_CUDA(cudaEventSynchronize(ev_[1]));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+        if (rep > 0) vbest = std::min(vbest, ms);
+      }
+      if (vbest < best_ms) {
+        best_ms = vbest;
+        best_v = v;
+      }
+    }
+    s = check_errors(db->plan, d);
+    delete db;
+    if (s != RODV_OK) return s;
+    variant_[c] = best_v;
+    if (opt_.verbose)
+      fprintf(stderr, "rodv: tuned class %d (R=%d%s%s): %d blocks/SM, %.3f ms\n", c, R,
+              uni ? ", uniform" : "", multi ? ", multi-pass" : "", kVariantMinBlocks[best_v],
+              best_ms);
+  }
+  tuned_ = true;
+  if (!path.empty()) save_tuning(path);
+  if (variants_out)
+    for (int c = 0; c < kNumClasses; ++c) variants_out[c] = variant_[c];
   return RODV_OK;
 }
 

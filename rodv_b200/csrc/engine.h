@@ -30,6 +30,18 @@ inline int class_rows(int cls) { return cls < kSinglePassClasses ? cls / 2 + 1 :
 inline bool class_uniform(int cls) { return (cls & 1) != 0; }
 inline bool class_multi(int cls) { return cls >= kSinglePassClasses; }
 
+// Device counters of one packed batch: per class the work counters of the
+// same-haplotype, two-haplotype and FP64 launches and the rescue count, then
+// one error word.
+enum CounterBlock : int {
+  kCtrSame = 0,
+  kCtrDiff = kNumClasses,
+  kCtrF64 = 2 * kNumClasses,
+  kCtrRescue = 3 * kNumClasses,
+  kCtrError = 4 * kNumClasses,
+  kCountWords = 4 * kNumClasses + 1,
+};
+
 struct DeviceMem {
   void* ptr = nullptr;
   size_t bytes = 0;
@@ -44,28 +56,31 @@ struct PinnedMem {
   cudaError_t ensure(size_t n);
 };
 
-// Host-side description of one packed batch (sizes and per-class counts).
+// Host-side description of one packed batch (sizes, per-class counts and the
+// byte offsets of every array in the staging buffer / device arena).
 struct PackedPlan {
   uint64_t num_pairs = 0, cells = 0;
   uint64_t hap_code_bytes = 0, read_rows = 0;
   uint32_t num_haps = 0, num_reads = 0;
   uint32_t max_hap_len = 0;
   uint32_t multi_max_hap = 0;
-  uint32_t items[kNumClasses] = {};      // FP32 items (pairs of pairs)
-  uint32_t pairs[kNumClasses] = {};      // pairs per class
-  // byte offsets inside the staging / device arena
-  size_t off_hap_codes = 0, off_read_rows = 0, off_haps = 0, off_reads = 0, off_pairs = 0;
-  size_t off_items[kNumClasses] = {};
-  size_t off_lists[kNumClasses] = {};    // FP64 work lists (rescue or forced)
-  size_t upload_bytes = 0;               // staging part: everything above
+  bool fp64 = false;                       // every pair computed in FP64
+  uint32_t same_items[kNumClasses] = {};   // FP32 same-haplotype items
+  uint32_t diff_items[kNumClasses] = {};   // FP32 two-haplotype items (leftovers)
+  uint32_t pairs[kNumClasses] = {};        // pairs per class
+  size_t off_hap_codes = 0, off_read_rows = 0, off_haps = 0, off_reads = 0;
+  size_t off_same[kNumClasses] = {};
+  size_t off_diff[kNumClasses] = {};
+  size_t off_lists[kNumClasses] = {};      // FP64 work lists (rescued or forced)
+  size_t upload_bytes = 0;                 // the H2D part starts at 0
   size_t off_out = 0, off_counts = 0, off_scratch = 0;
   size_t total_bytes = 0;
   size_t scratch_bytes = 0;
   uint32_t scratch_cols = 0;
-  bool fp64 = false;                     // every pair computed in FP64
+  // host copies kept for the plain per-pair form
+  std::vector<rodv_region> regions;
+  std::vector<uint8_t> read_class;
 };
-
-struct rodv_device_batch_impl;
 
 class Engine {
  public:
@@ -79,6 +94,7 @@ class Engine {
   rodv_status download(rodv_device_batch* db, double* out);
   rodv_status plain(rodv_device_batch* db, double* out, rodv_stats* st);
   rodv_status measure_peaks(double* f32, double* f32x2, double* f64, double* mhz);
+  rodv_status autotune(const char* cache_path, int force, int32_t* variants_out);
 
   std::mutex& mutex() { return mu_; }
   const char* last_error() const { return last_error_.c_str(); }
@@ -88,16 +104,24 @@ class Engine {
  private:
   rodv_status pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64);
   rodv_status launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stats* st, bool timed);
+  rodv_status launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, int cls, bool same,
+                                int variant, int blocks_cap);
   rodv_status check_errors(const PackedPlan& plan, uint8_t* dbase);
   int persistent_blocks(const KernelInfo& k) const;
+  std::string device_key() const;
+  bool load_tuning(const std::string& path);
+  bool save_tuning(const std::string& path) const;
 
   rodv_options opt_;
   int device_ = 0;
   int num_sms_ = 0;
+  std::string device_name_;
   cudaStream_t stream_ = nullptr;
   cudaEvent_t ev_[4] = {};
   DeviceMem tables_;
   PriorTables tab_{};
+  int variant_[kNumClasses] = {};          // tuned occupancy variant per class
+  bool tuned_ = false;
   // buffers of the one-call path (rodv_pairhmm_batch), reused across calls
   PinnedMem staging_;
   PinnedMem out_staging_;

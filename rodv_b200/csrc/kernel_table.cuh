@@ -1,0 +1,54 @@
+// kernel_table.cuh -- KernelInfo of every forward-kernel instantiation.
+//
+// Each rows-per-lane value R is instantiated in its own translation unit
+// (kernels_r<R>.cu, kernels_multi.cu) so the ~100 kernels compile in parallel.
+#pragma once
+#include <type_traits>
+
+#include "kernels.h"
+#include "pairhmm_fwd.cuh"
+
+namespace rodv {
+
+template <class P, int R, bool U, bool MU, bool SAME, int MINB>
+KernelInfo make_info(int variant) {
+  using F = Forward<P, R, U, MU, SAME, MINB>;
+  KernelInfo k;
+  k.fn = reinterpret_cast<const void*>(&forward_kernel<P, R, U, MU, SAME, MINB>);
+  k.threads = F::kWarpsPerBlock * kWarp;
+  k.warps_per_block = F::kWarpsPerBlock;
+  k.smem_bytes = F::kWarpsPerBlock * TableShape<P, R, SAME>::kBytesPerWarp;
+  k.rows_per_lane = R;
+  k.multi = MU;
+  k.same_hap = SAME || P::kSlots == 1;
+  k.min_blocks = MINB;
+  k.variant = variant;
+  return k;
+}
+
+// Same-haplotype FP32 kernels come in kTuneVariants occupancy targets
+// (kVariantMinBlocks); every other kernel has one variant.
+template <class P, int R, bool U, bool MU, bool SAME>
+KernelInfo variant_info(int variant) {
+  if (!(std::is_same<P, F32x2>::value && SAME)) return make_info<P, R, U, MU, SAME, 1>(0);
+  switch (variant) {
+    case 0: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[0]>(0);
+    case 1: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[1]>(1);
+    case 2: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[2]>(2);
+    default: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[3]>(3);
+  }
+}
+
+template <int R, bool MU>
+KernelInfo info_for(Precision prec, bool uniform, bool same, int variant) {
+  if (prec == Precision::kF64)
+    return uniform ? variant_info<F64, R, true, MU, false>(0)
+                   : variant_info<F64, R, false, MU, false>(0);
+  if (same)
+    return uniform ? variant_info<F32x2, R, true, MU, true>(variant)
+                   : variant_info<F32x2, R, false, MU, true>(variant);
+  return uniform ? variant_info<F32x2, R, true, MU, false>(0)
+                 : variant_info<F32x2, R, false, MU, false>(0);
+}
+
+}  // namespace rodv

@@ -13,11 +13,24 @@ struct KernelInfo {
   int smem_bytes = 0;         // dynamic shared memory per block
   int rows_per_lane = 0;      // R
   bool multi = false;         // sweeps reads longer than 32*R rows in passes
+  bool same_hap = false;      // both pairs of an item share the haplotype
+  int min_blocks = 1;         // launch-bounds occupancy target (caps registers)
+  int variant = 0;
 };
 
+// Occupancy targets of the tunable (same-haplotype FP32) kernels.
+constexpr int kTuneVariants = 4;
+constexpr int kVariantMinBlocks[kTuneVariants] = {4, 5, 6, 8};
+
 // Forward kernel for one work class.  rows_per_lane in 1..8; multi kernels
-// always use 8 rows per lane.
-KernelInfo forward_kernel_info(Precision prec, int rows_per_lane, bool uniform, bool multi);
+// always use 8 rows per lane.  same: items whose two pairs share the
+// haplotype (FP32 only; FP64 items hold one pair).  variant < kTuneVariants
+// selects the occupancy target of same-haplotype FP32 kernels.
+KernelInfo forward_kernel_info(Precision prec, int rows_per_lane, bool uniform, bool multi,
+                               bool same = true, int variant = 0);
+inline int forward_kernel_variants(Precision prec, bool same) {
+  return (prec == Precision::kF32x2 && same) ? kTuneVariants : 1;
+}
 
 // Peak microbenchmarks: kind 0 = FP32 FFMA, 1 = FP32x2 FFMA2, 2 = FP64 DFMA.
 // scratch must hold kPeakScratchBytes; the FFMA run stores the SM cycles its

@@ -12,13 +12,22 @@
 //                     24-30 gcp (quals masked with &127 as the reference
 //                     does, pairhmm_inter.cpp:85-88); each read starts on a
 //                     16-byte boundary.
-//   haps       HapDesc[], reads ReadDesc[], pairs PairDesc[]
-//   items      Item[]  the FP32 kernel's work: two pairs per warp (the two
-//                      float lanes of every packed f32x2 instruction)
+//   haps       HapDesc[], reads ReadDesc[]
+//   items      the FP32 kernels' work, two pairs per warp (the two float
+//              halves of every f32x2 instruction): SameItem (two reads against
+//              one haplotype) or a DiffItem (two PairRef) for the leftovers
+//   lists      PairRef[] per work class: the FP64 kernels' work (pairs the
+//              FP32 kernels rescued, or every pair when FP64 is forced)
 //   out        f64[num_pairs]  final log10 likelihood, in the reference's
-//                              result order (region, hap-major, read-minor)
+//              result order (region, hap-major, read-minor)
 #pragma once
 #include <cstdint>
+
+#if defined(__CUDACC__)
+#define RODV_HD __host__ __device__
+#else
+#define RODV_HD
+#endif
 
 namespace rodv {
 
@@ -45,29 +54,40 @@ struct ReadDesc {
 };
 constexpr uint32_t kReadUniformGaps = 1u;
 
-struct PairDesc {
+// One (haplotype, read) pair and where its result goes.
+struct PairRef {
   uint32_t hap;
-  uint32_t read;
-  uint64_t out;       // index in the output array
+  uint32_t read;      // kNoPair marks an empty slot
+  uint32_t out;       // index in the output array
 };
 
-// Two pairs computed together by one warp.  Slot x is the pair with the
-// longer (or equal) haplotype; y may be kNoPair.
-struct Item {
-  uint32_t x;
-  uint32_t y;
+// Two reads of one region against one haplotype.  The result index of read y
+// is out_x + (read_y - read_x): reads of a region are contiguous and results
+// are hap-major.  read_y may be kNoPair.
+struct SameItem {
+  uint32_t hap;
+  uint32_t read_x;
+  uint32_t read_y;
+  uint32_t out_x;
 };
 
-__host__ __device__ inline uint32_t row_word(uint32_t code, uint32_t q, uint32_t ins,
+// Two arbitrary pairs; x has the longer (or equal) haplotype; y.read may be
+// kNoPair.
+struct DiffItem {
+  PairRef x;
+  PairRef y;
+};
+
+RODV_HD inline uint32_t row_word(uint32_t code, uint32_t q, uint32_t ins,
                                              uint32_t del, uint32_t gcp) {
   return (code & 7u) | ((q & 127u) << 3) | ((ins & 127u) << 10) | ((del & 127u) << 17) |
          ((gcp & 127u) << 24);
 }
-__host__ __device__ inline uint32_t rw_code(uint32_t w) { return w & 7u; }
-__host__ __device__ inline uint32_t rw_q(uint32_t w) { return (w >> 3) & 127u; }
-__host__ __device__ inline uint32_t rw_ins(uint32_t w) { return (w >> 10) & 127u; }
-__host__ __device__ inline uint32_t rw_del(uint32_t w) { return (w >> 17) & 127u; }
-__host__ __device__ inline uint32_t rw_gcp(uint32_t w) { return (w >> 24) & 127u; }
+RODV_HD inline uint32_t rw_code(uint32_t w) { return w & 7u; }
+RODV_HD inline uint32_t rw_q(uint32_t w) { return (w >> 3) & 127u; }
+RODV_HD inline uint32_t rw_ins(uint32_t w) { return (w >> 10) & 127u; }
+RODV_HD inline uint32_t rw_del(uint32_t w) { return (w >> 17) & 127u; }
+RODV_HD inline uint32_t rw_gcp(uint32_t w) { return (w >> 24) & 127u; }
 
 // Prior tables in the two precisions (Context<float>/Context<double>,
 // context.h:22-166): ph2pr[q] and the match-to-match table indexed by
@@ -86,18 +106,17 @@ struct BatchView {
   const uint32_t* read_rows;
   const HapDesc* haps;
   const ReadDesc* reads;
-  const PairDesc* pairs;
   double* out;
   PriorTables tab;
 };
 
 // One launch of a forward kernel over one class of work.
 struct ClassLaunch {
-  const uint32_t* work;        // FP32: Item list (2 words per item); FP64: pair list
+  const void* work;            // SameItem[] / DiffItem[] (FP32) or PairRef[] (FP64)
   const uint32_t* work_count;  // device count (FP64 rescue lists) or null
   uint32_t static_count;       // item count when work_count is null
   uint32_t* counter;           // work counter, zeroed before launch
-  uint32_t* rescue_list;       // FP32 only: pairs whose result fell below 1e-28
+  PairRef* rescue_list;        // FP32 only: pairs whose result fell below 1e-28
   uint32_t* rescue_count;
   float* scratch;              // MULTI: per resident warp boundary-row buffer
   uint32_t scratch_cols;       // columns per warp buffer (max hap len + 40)

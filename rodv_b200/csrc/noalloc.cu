@@ -18,7 +18,7 @@
 // device memory, and a device output array.  On the caller's stream:
 //   na_prefix_kernel   validates sizes and computes offsets (one block);
 //   na_pack_kernel     packs bases and qualities into the scratch layout;
-//   na_pairs_kernel    builds pair descriptors and two-pair work items;
+//   na_pairs_kernel    builds the two-pair work items (and FP64 lists);
 //   forward_kernel     the multi-pass FP32 kernel (8 rows per lane, per-row
 //                      gap priors) and its FP64 rescue -- the same kernel
 //                      template as the batched engine -- with the boundary rows
@@ -78,10 +78,9 @@ constexpr size_t kOffHaps = al(kOffHapCodes + kHapCodeUsedMax + kHapTail);
 constexpr size_t kOffRows = al(kOffHaps + kNaMaxHaps * sizeof(HapDesc));
 constexpr size_t kRowWords = kNaMaxReadBases + 3 * (size_t)kNaMaxReads;
 constexpr size_t kOffReads = al(kOffRows + kRowWords * 4);
-constexpr size_t kOffPairs = al(kOffReads + kNaMaxReads * sizeof(ReadDesc));
-constexpr size_t kOffItems = al(kOffPairs + kNaMaxPairs * sizeof(PairDesc));
-constexpr size_t kOffList = al(kOffItems + (kNaMaxPairs / 2 + 1) * sizeof(Item));
-constexpr size_t kOffBoundary = al(kOffList + kNaMaxPairs * 4);
+constexpr size_t kOffItems = al(kOffReads + kNaMaxReads * sizeof(ReadDesc));
+constexpr size_t kOffList = al(kOffItems + (kNaMaxPairs / 2 + 1) * sizeof(DiffItem));
+constexpr size_t kOffBoundary = al(kOffList + kNaMaxPairs * sizeof(PairRef));
 constexpr size_t kScratchBytes = al(kOffBoundary + (size_t)kNaWarps * kNaCols * 24);
 
 // counter words
@@ -264,54 +263,44 @@ __global__ void na_pack_kernel(NaArgs a) {
   if (err) atomicOr(&c[kCErr], err);
 }
 
-// Pair descriptors in result order, two-pair FP32 items (longer haplotype in
-// slot x), and the FP64 list when every pair is forced to FP64.
+// Pair p (result order) as a PairRef: its region by binary search over the
+// region offsets, then hap-major position inside the region.
+__device__ __forceinline__ PairRef pair_ref(const NaArgs& a, uint32_t p) {
+  const unsigned long long* reg_off =
+      reinterpret_cast<const unsigned long long*>(a.s + kOffRegOff);
+  uint32_t lo = 0, hi = a.b.num_regions;  // reg_off[lo] <= p < reg_off[hi]
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) / 2;
+    if (reg_off[mid] <= p) lo = mid; else hi = mid;
+  }
+  const rodv_region r = a.b.regions[lo];
+  const uint32_t local = p - (uint32_t)reg_off[lo];
+  return PairRef{r.hap_start + local / r.num_reads, r.read_start + local % r.num_reads, p};
+}
+
+// Two-pair FP32 items over consecutive pairs (longer haplotype in slot x),
+// and the FP64 list when every pair is forced to FP64.
 __global__ void na_pairs_kernel(NaArgs a) {
   uint32_t* c = counters(a.s);
   const uint32_t np = c[kCPairs];
-  const rodv_batch& b = a.b;
-  const unsigned long long* reg_off =
-      reinterpret_cast<const unsigned long long*>(a.s + kOffRegOff);
-  PairDesc* pd = reinterpret_cast<PairDesc*>(a.s + kOffPairs);
-  Item* items = reinterpret_cast<Item*>(a.s + kOffItems);
-  uint32_t* list = reinterpret_cast<uint32_t*>(a.s + kOffList);
+  DiffItem* items = reinterpret_cast<DiffItem*>(a.s + kOffItems);
+  PairRef* list = reinterpret_cast<PairRef*>(a.s + kOffList);
   const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += stride) {
-    uint32_t lo = 0, hi = b.num_regions;  // reg_off[lo] <= p < reg_off[hi]
-    while (hi - lo > 1) {
-      const uint32_t mid = (lo + hi) / 2;
-      if (reg_off[mid] <= p) lo = mid; else hi = mid;
-    }
-    const rodv_region r = b.regions[lo];
-    const uint32_t local = p - (uint32_t)reg_off[lo];
-    pd[p].hap = r.hap_start + local / r.num_reads;
-    pd[p].read = r.read_start + local % r.num_reads;
-    pd[p].out = p;
-    if (a.use_double) list[p] = p;
-  }
+  if (a.use_double)
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += stride)
+      list[p] = pair_ref(a, p);
   const uint32_t ni = c[kCItems];
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < ni; k += stride) {
-    // the hap of pair p, recomputed (pd[] of another thread may not be written yet)
-    auto hap_len_of = [&](uint32_t p) {
-      uint32_t lo = 0, hi = b.num_regions;
-      while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) / 2;
-        if (reg_off[mid] <= p) lo = mid; else hi = mid;
-      }
-      const rodv_region r = b.regions[lo];
-      return b.hap_lengths[r.hap_start + (p - (uint32_t)reg_off[lo]) / r.num_reads];
-    };
-    const uint32_t x = 2 * k, y = 2 * k + 1;
-    if (y >= np) {
+    const PairRef x = pair_ref(a, 2 * k);
+    if (2 * k + 1 >= np) {
       items[k].x = x;
-      items[k].y = kNoPair;
-    } else if (hap_len_of(x) >= hap_len_of(y)) {
-      items[k].x = x;
-      items[k].y = y;
-    } else {
-      items[k].x = y;
-      items[k].y = x;
+      items[k].y = PairRef{0, kNoPair, 0};
+      continue;
     }
+    const PairRef y = pair_ref(a, 2 * k + 1);
+    const bool swap = a.b.hap_lengths[y.hap] > a.b.hap_lengths[x.hap];
+    items[k].x = swap ? y : x;
+    items[k].y = swap ? x : y;
   }
 }
 
@@ -395,7 +384,6 @@ extern "C" rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32
   v.read_rows = reinterpret_cast<const uint32_t*>(s + kOffRows);
   v.haps = reinterpret_cast<const HapDesc*>(s + kOffHaps);
   v.reads = reinterpret_cast<const ReadDesc*>(s + kOffReads);
-  v.pairs = reinterpret_cast<const PairDesc*>(s + kOffPairs);
   v.out = out_log10;
   v.tab.ph2pr_f = reinterpret_cast<const float*>(s + kOffPh2prF);
   v.tab.mm_f = reinterpret_cast<const float*>(s + kOffMmF);
@@ -403,29 +391,31 @@ extern "C" rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32
   v.tab.mm_d = reinterpret_cast<const double*>(s + kOffMmD);
   uint32_t* cnt = reinterpret_cast<uint32_t*>(s + kOffCounters);
 
-  using F32 = Forward<F32x2, kMaxRowsPerLane, false, true>;
-  using D64 = Forward<F64, kMaxRowsPerLane, false, true>;
+  using F32 = Forward<F32x2, kMaxRowsPerLane, false, true, false, 1>;
+  using D64 = Forward<F64, kMaxRowsPerLane, false, true, false, 1>;
   ClassLaunch c32{};
-  c32.work = reinterpret_cast<const uint32_t*>(s + kOffItems);
+  c32.work = s + kOffItems;
   c32.work_count = cnt + kCItems;
   c32.counter = cnt + kCCtr32;
-  c32.rescue_list = reinterpret_cast<uint32_t*>(s + kOffList);
+  c32.rescue_list = reinterpret_cast<PairRef*>(s + kOffList);
   c32.rescue_count = cnt + kCRescue;
   c32.scratch = reinterpret_cast<float*>(s + kOffBoundary);
   c32.scratch_cols = kNaCols;
   c32.error_flags = cnt + kCErr;
-  forward_kernel<F32x2, kMaxRowsPerLane, false, true>
+  forward_kernel<F32x2, kMaxRowsPerLane, false, true, false, 1>
       <<<kNaBlocks, F32::kWarpsPerBlock * kWarp,
-         F32::kWarpsPerBlock * TableShape<F32x2, kMaxRowsPerLane>::kBytesPerWarp, st>>>(v, c32);
+         F32::kWarpsPerBlock * TableShape<F32x2, kMaxRowsPerLane, false>::kBytesPerWarp, st>>>(
+          v, c32);
   ClassLaunch c64 = c32;
-  c64.work = reinterpret_cast<const uint32_t*>(s + kOffList);
+  c64.work = s + kOffList;
   c64.work_count = cnt + kCRescue;
   c64.counter = cnt + kCCtr64;
   c64.rescue_list = nullptr;
   c64.rescue_count = nullptr;
-  forward_kernel<F64, kMaxRowsPerLane, false, true>
+  forward_kernel<F64, kMaxRowsPerLane, false, true, false, 1>
       <<<kNaBlocks, D64::kWarpsPerBlock * kWarp,
-         D64::kWarpsPerBlock * TableShape<F64, kMaxRowsPerLane>::kBytesPerWarp, st>>>(v, c64);
+         D64::kWarpsPerBlock * TableShape<F64, kMaxRowsPerLane, false>::kBytesPerWarp, st>>>(
+          v, c64);
   if (cudaGetLastError() != cudaSuccess) return RODV_ERR_CUDA;
 
   uint32_t flags = 0;

@@ -29,7 +29,7 @@
 // Emission.  e(i,j) depends on the read base of row i and the haplotype base
 // of column j.  Each lane keeps, in shared memory, a table E[code][k] of its
 // rows' emissions for each of the five haplotype codes, laid out so that the
-// per-step load of R values is a conflict-free 16-byte vector load per lane.
+// per-step loads are conflict-free 16-byte vector loads.
 //
 // Precision policies.  F32x2 packs two independent pairs into the two halves
 // of the sm_100 f32x2 instructions (__ffma2_rn / __fadd2_rn / __fmul2_rn), so
@@ -38,12 +38,24 @@
 // the reference's acceptance threshold (MIN_ACCEPTED 1e-28,
 // pairhmm/intra/pairhmm_api.cpp:4-23, pairhmm_schedule.cpp:229-248).
 //
+// Item shapes (F32x2).  SAME: both pairs share the haplotype (two reads of
+// one region against one haplotype): one code load per step, the two slots'
+// emissions interleaved in the table so that every row's pair of emissions is
+// one f32x2 operand, and every FP32 instruction of the step is an f32x2
+// instruction (a scalar FP32 instruction holds one half of the FMA pipe and
+// stalls the next f32x2 one).  DIFF: any two pairs (the leftovers of SAME
+// pairing); separate per-slot tables, scalar emission multiplies, and the
+// shorter haplotype's running sum frozen when its last column has passed.
+//
 // Uniform-gap form.  When a read's ins/del/gcp quals are constant (GATK data,
 // and every benchmark config), the kernel stores M~ = M/gapm instead of M:
 //   M~ = e*(mm*M~_d + I_d + D_d),  I = (mi*gapm)*M~_u + ii*I_u,
 //   D = (md*gapm)*M~_l + dd*D_l
 // which is 7 arithmetic instructions per cell instead of 8.  The result is
 // gapm*sum(M~) + sum(I).
+//
+// MINB is the launch-bounds occupancy target (blocks per SM); it caps the
+// registers per thread and is chosen per work class by the autotuner.
 #pragma once
 #include <cuda_runtime.h>
 #include <math_constants.h>
@@ -66,7 +78,6 @@ struct F32x2 {
   using V = float2;
   using S = float;
   static constexpr int kSlots = 2;
-  static constexpr int kVec = 4;  // table entries per 16-byte load
   __device__ __forceinline__ static V add(V a, V b) { return __fadd2_rn(a, b); }
   __device__ __forceinline__ static V mul(V a, V b) { return __fmul2_rn(a, b); }
   __device__ __forceinline__ static V fma(V a, V b, V c) { return __ffma2_rn(a, b, c); }
@@ -85,7 +96,6 @@ struct F64 {
   using V = double;
   using S = double;
   static constexpr int kSlots = 1;
-  static constexpr int kVec = 2;
   __device__ __forceinline__ static V add(V a, V b) { return a + b; }
   __device__ __forceinline__ static V mul(V a, V b) { return a * b; }
   __device__ __forceinline__ static V fma(V a, V b, V c) { return __fma_rn(a, b, c); }
@@ -95,7 +105,9 @@ struct F64 {
   __device__ __forceinline__ static S sx(V v) { return v; }
   __device__ __forceinline__ static S sy(V v) { return v; }
   // 2^1020, Context<double>::INITIAL_CONSTANT (context.h:101)
-  __device__ __forceinline__ static S init_const() { return __longlong_as_double(0x7fb0000000000000ll); }
+  __device__ __forceinline__ static S init_const() {
+    return __longlong_as_double(0x7fb0000000000000ll);
+  }
 };
 
 template <class S>
@@ -134,12 +146,21 @@ __device__ __forceinline__ RowPriors<S> row_priors(uint32_t w, const PriorTables
   return p;
 }
 
-// Shared-memory bytes of one warp's emission tables for R rows per lane.
-template <class P, int R>
+// Shared-memory shape of one warp's emission tables for R rows per lane.
+//   SAME layout (F64 always, F32x2 same-haplotype items): element (code, k)
+//     is one V; a 16-byte vector holds rows k, k+1 of the lane:
+//     vec index ((code * kNv + k/2) * 32 + lane).
+//   DIFF layout (F32x2 two-haplotype items): per slot, element (slot, code, k)
+//     is one float; a 16-byte vector holds rows k..k+3 of the lane:
+//     vec index (((slot * 5 + code) * kNv + k/4) * 32 + lane).
+template <class P, int R, bool SAME>
 struct TableShape {
-  static constexpr int kRq = (R + P::kVec - 1) / P::kVec * P::kVec;   // rows, padded
-  static constexpr int kNv = kRq / P::kVec;                          // 16-byte loads per slot
-  static constexpr int kBytesPerWarp = P::kSlots * 5 * kRq * kWarp * (int)sizeof(typename P::S);
+  static constexpr bool kSameLayout = SAME || P::kSlots == 1;
+  static constexpr int kRowsPerVec = kSameLayout ? 2 : 4;
+  static constexpr int kRq = (R + kRowsPerVec - 1) / kRowsPerVec * kRowsPerVec;
+  static constexpr int kNv = kRq / kRowsPerVec;  // 16-byte loads per code (per slot)
+  static constexpr int kTables = kSameLayout ? 1 : 2;
+  static constexpr int kBytesPerWarp = kTables * 5 * kNv * kWarp * 16;
 };
 
 // Per-slot state of the pair being computed.
@@ -147,16 +168,16 @@ struct SlotInfo {
   const uint8_t* hap;   // first base code of the haplotype
   uint32_t H, L;
   uint64_t row_off;
-  uint64_t out;
-  uint32_t pair;
+  PairRef ref;
   bool valid;
 };
 
-template <class P, int R, bool UNIFORM, bool MULTI>
+template <class P, int R, bool UNIFORM, bool MULTI, bool SAME, int MINB>
 struct Forward {
   using V = typename P::V;
   using S = typename P::S;
-  using Shape = TableShape<P, R>;
+  using Shape = TableShape<P, R, SAME>;
+  static constexpr bool kSameHap = Shape::kSameLayout;
   static constexpr int kWarpsPerBlock = 4;
 
   // Boundary row written by lane 31 of one pass and read by lane 0 of the next.
@@ -164,35 +185,53 @@ struct Forward {
     V m, i, d;
   };
 
+  // Writes emission e of (slot, code, row k) into this lane's table.
+  __device__ __forceinline__ static void put_emission(S* tab, int slot, int code, int k, int lane,
+                                                      S e) {
+    if (kSameHap) {
+      const int vec = (code * Shape::kNv + k / 2) * kWarp + lane;
+      // 16-byte vector = 2 rows of V; V = S[kSlots]
+      tab[vec * (16 / (int)sizeof(S)) + (k % 2) * P::kSlots + slot] = e;
+    } else {
+      const int vec = ((slot * 5 + code) * Shape::kNv + k / 4) * kWarp + lane;
+      tab[vec * 4 + (k % 4)] = e;
+    }
+  }
+
   __device__ static void run_item(const BatchView& b, const ClassLaunch& c, uint32_t item,
                                   int lane, int gwarp, uint4* table) {
-    SlotInfo sl[2];
-    uint32_t pair_ids[2];
-    if (P::kSlots == 2) {
-      pair_ids[0] = c.work[2 * item];
-      pair_ids[1] = c.work[2 * item + 1];
+    PairRef refs[2];
+    if (P::kSlots == 1) {
+      refs[0] = static_cast<const PairRef*>(c.work)[item];
+      refs[1] = refs[0];
+      refs[1].read = kNoPair;
+    } else if (SAME) {
+      const SameItem it = static_cast<const SameItem*>(c.work)[item];
+      refs[0] = PairRef{it.hap, it.read_x, it.out_x};
+      refs[1] = PairRef{it.hap, it.read_y, it.out_x + (it.read_y - it.read_x)};
     } else {
-      pair_ids[0] = c.work[item];
-      pair_ids[1] = kNoPair;
+      const DiffItem it = static_cast<const DiffItem*>(c.work)[item];
+      refs[0] = it.x;
+      refs[1] = it.y;
     }
+    SlotInfo sl[2];
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
-      const uint32_t pid = (s == 1 && pair_ids[1] == kNoPair) ? pair_ids[0] : pair_ids[s];
-      const PairDesc pd = b.pairs[pid];
-      const HapDesc hd = b.haps[pd.hap];
-      const ReadDesc rd = b.reads[pd.read];
+      const bool valid = (s == 0) || refs[1].read != kNoPair;
+      const PairRef r = valid ? refs[s] : refs[0];
+      const HapDesc hd = b.haps[r.hap];
+      const ReadDesc rd = b.reads[r.read];
       sl[s].hap = b.hap_codes + hd.code_off;
       sl[s].H = hd.len;
       sl[s].L = rd.len;
       sl[s].row_off = rd.row_off;
-      sl[s].out = pd.out;
-      sl[s].pair = pid;
-      sl[s].valid = (s == 0) || (pair_ids[1] != kNoPair);
+      sl[s].ref = r;
+      sl[s].valid = valid;
     }
     const uint32_t Lmax = sl[0].L > sl[1].L ? sl[0].L : sl[1].L;
     const uint32_t passes = MULTI ? (Lmax + kWarp * R - 1) / (kWarp * R) : 1;
     if (sl[0].H == 0 || sl[1].H == 0 || sl[0].L == 0 || sl[1].L == 0 ||
-        (!MULTI && Lmax > (uint32_t)(kWarp * R)) ||
+        (kSameHap && sl[0].hap != sl[1].hap) || (!MULTI && Lmax > (uint32_t)(kWarp * R)) ||
         (MULTI && (uint64_t)sl[0].H + 40 > c.scratch_cols)) {
       if (lane == 0) atomicOr(c.error_flags, kErrBadLength);
       return;
@@ -202,8 +241,8 @@ struct Forward {
     const V init = P::make(P::init_const() / (S)sl[0].H, P::init_const() / (S)sl[1].H);
 
     // Uniform-gap priors come from the read's first row.
-    RowPriors<S> u0 = row_priors<S>(b.read_rows[sl[0].row_off], b.tab);
-    RowPriors<S> u1 = row_priors<S>(b.read_rows[sl[1].row_off], b.tab);
+    const RowPriors<S> u0 = row_priors<S>(b.read_rows[sl[0].row_off], b.tab);
+    const RowPriors<S> u1 = row_priors<S>(b.read_rows[sl[1].row_off], b.tab);
     const V gapmU = P::make(u0.gapm, u1.gapm);
     const V mmU = P::make(u0.mm, u1.mm);
     const V mdU = P::make(u0.md * u0.gapm, u1.md * u1.gapm);
@@ -234,11 +273,7 @@ struct Forward {
 #pragma unroll
           for (int code = 0; code < 5; ++code) {
             const bool hit = (rc == (uint32_t)code) || rc == kN || code == kN;
-            const S e = real ? (hit ? rp.match : rp.mismatch) : S(0);
-            // element (slot, code, k) of this lane's table
-            const int idx = (((s * 5 + code) * Shape::kNv + k / P::kVec) * kWarp + lane) * P::kVec +
-                            (k % P::kVec);
-            tab[idx] = e;
+            put_emission(tab, s, code, k, lane, real ? (hit ? rp.match : rp.mismatch) : S(0));
           }
           if (UNIFORM) {
             const RowPriors<S>& up = (s == 0) ? u0 : u1;
@@ -291,28 +326,36 @@ struct Forward {
           }
         }
         // emission values of this lane's rows for its current column
-        S ex[Shape::kRq], ey[Shape::kRq];
-        {
+        V e[R];
+        if (kSameHap) {
           const uint32_t cx = hx[s];
           const uint4* px = tab_x + cx * (Shape::kNv * kWarp);
 #pragma unroll
           for (int v = 0; v < Shape::kNv; ++v) {
             const uint4 raw = px[v * kWarp];
-            const S* f = reinterpret_cast<const S*>(&raw);
-#pragma unroll
-            for (int e = 0; e < P::kVec; ++e) ex[v * P::kVec + e] = f[e];
+            const V* f = reinterpret_cast<const V*>(&raw);
+            if (2 * v < R) e[2 * v] = f[0];
+            if (2 * v + 1 < R) e[2 * v + 1] = f[1];
           }
-          if (P::kSlots == 2) {
-            const uint32_t cy = hy[s];
-            const uint4* py = tab_y + cy * (Shape::kNv * kWarp);
+        } else {
+          S ex[Shape::kRq], ey[Shape::kRq];
+          const uint32_t cx = hx[s];
+          const uint4* px = tab_x + cx * (Shape::kNv * kWarp);
+          const uint32_t cy = hy[s];
+          const uint4* py = tab_y + cy * (Shape::kNv * kWarp);
 #pragma unroll
-            for (int v = 0; v < Shape::kNv; ++v) {
-              const uint4 raw = py[v * kWarp];
-              const S* f = reinterpret_cast<const S*>(&raw);
+          for (int v = 0; v < Shape::kNv; ++v) {
+            const uint4 rx = px[v * kWarp], ry = py[v * kWarp];
+            const S* fx = reinterpret_cast<const S*>(&rx);
+            const S* fy = reinterpret_cast<const S*>(&ry);
 #pragma unroll
-              for (int e = 0; e < P::kVec; ++e) ey[v * P::kVec + e] = f[e];
+            for (int q = 0; q < 4; ++q) {
+              ex[v * 4 + q] = fx[q];
+              ey[v * 4 + q] = fy[q];
             }
           }
+#pragma unroll
+          for (int k = 0; k < R; ++k) e[k] = P::make(ex[k], ey[k]);
         }
         V dm = dg_m, di = dg_i, dd = dg_d, um = up_m, ui = up_i;
 #pragma unroll
@@ -325,10 +368,10 @@ struct Forward {
             t = P::mul(pgapm[k], t);
             t = P::fma(pmm[k], dm, t);
           }
-          if (P::kSlots == 2) {
-            M[k] = P::make(P::sx(t) * ex[k], P::sy(t) * ey[k]);
+          if (kSameHap) {
+            M[k] = P::mul(t, e[k]);
           } else {
-            M[k] = P::mul(t, P::make(ex[k], ex[k]));
+            M[k] = P::make(P::sx(t) * P::sx(e[k]), P::sy(t) * P::sy(e[k]));
           }
           I[k] = P::fma(pii[k], ui, P::mul(pmi[k], um));
           if (UNIFORM) {
@@ -351,7 +394,7 @@ struct Forward {
         if (last) {
           acc_m = P::add(acc_m, M[R - 1]);
           acc_i = P::add(acc_i, I[R - 1]);
-          if (P::kSlots == 2 && s == nfreeze - 1) {
+          if (P::kSlots == 2 && !kSameHap && s == nfreeze - 1) {
             frozen_m = P::sy(acc_m);
             frozen_i = P::sy(acc_i);
           }
@@ -361,6 +404,10 @@ struct Forward {
     }
 
     if (lane != kWarp - 1) return;
+    if (P::kSlots == 2 && kSameHap) {  // both slots ran exactly their own columns
+      frozen_m = P::sy(acc_m);
+      frozen_i = P::sy(acc_i);
+    }
     S res[2];
     res[0] = UNIFORM ? P::sx(gapmU) * P::sx(acc_m) + P::sx(acc_i) : P::sx(acc_m) + P::sx(acc_i);
     if (P::kSlots == 2)
@@ -372,38 +419,35 @@ struct Forward {
     }
   }
 
+  // FP32 result: accepted at >= 1e-28 with an FP64 log10, else queued for FP64.
   __device__ static void finish(const BatchView& b, const ClassLaunch& c, const SlotInfo& sl,
-                                S raw);
+                                S raw) {
+    if (P::kSlots == 2) {
+      if (raw >= kMinAcceptedF) {
+        b.out[sl.ref.out] = log10((double)raw) - kLog10InitF;
+      } else {
+        const uint32_t k = atomicAdd(c.rescue_count, 1u);
+        c.rescue_list[k] = sl.ref;
+      }
+    } else {
+      // The reference computes with flush-to-zero on (common.h:58-62), which on
+      // x86 also flushes FP64 denormals: a likelihood below the normal FP64
+      // range of the 2^1020 scaling becomes 0 and its log10 is -inf.  The GPU's
+      // FP64 keeps denormals, so such a result is mapped to -inf here.
+      b.out[sl.ref.out] = (raw >= kDblMin) ? log10((double)raw) - kLog10InitD : -CUDART_INF;
+    }
+  }
 };
 
-// FP32 result: accept at >= 1e-28 with an FP64 log10, else queue for FP64.
-template <class P, int R, bool UNIFORM, bool MULTI>
-__device__ void Forward<P, R, UNIFORM, MULTI>::finish(const BatchView& b, const ClassLaunch& c,
-                                                      const SlotInfo& sl, S raw) {
-  if (P::kSlots == 2) {
-    if (raw >= kMinAcceptedF) {
-      b.out[sl.out] = log10((double)raw) - kLog10InitF;
-    } else {
-      const uint32_t k = atomicAdd(c.rescue_count, 1u);
-      c.rescue_list[k] = sl.pair;
-    }
-  } else {
-    // The reference computes with flush-to-zero on (common.h:58-62), which on
-    // x86 also flushes FP64 denormals: a likelihood below the normal FP64
-    // range of the 2^1020 scaling becomes 0 and its log10 is -inf.  The GPU's
-    // FP64 keeps denormals, so such a result is mapped to -inf here.
-    b.out[sl.out] = (raw >= kDblMin) ? log10((double)raw) - kLog10InitD : -CUDART_INF;
-  }
-}
-
-template <class P, int R, bool UNIFORM, bool MULTI>
-__global__ void __launch_bounds__(Forward<P, R, UNIFORM, MULTI>::kWarpsPerBlock * kWarp)
+template <class P, int R, bool UNIFORM, bool MULTI, bool SAME, int MINB>
+__global__ void __launch_bounds__(Forward<P, R, UNIFORM, MULTI, SAME, MINB>::kWarpsPerBlock * kWarp,
+                                  MINB)
     forward_kernel(BatchView b, ClassLaunch c) {
-  using F = Forward<P, R, UNIFORM, MULTI>;
+  using F = Forward<P, R, UNIFORM, MULTI, SAME, MINB>;
   extern __shared__ uint4 smem[];
   const int lane = threadIdx.x & (kWarp - 1);
   const int warp = threadIdx.x / kWarp;
-  uint4* table = smem + warp * (TableShape<P, R>::kBytesPerWarp / 16);
+  uint4* table = smem + warp * (TableShape<P, R, SAME>::kBytesPerWarp / 16);
   const int gwarp = blockIdx.x * F::kWarpsPerBlock + warp;
   const uint32_t n = c.work_count ? *c.work_count : c.static_count;
   for (;;) {

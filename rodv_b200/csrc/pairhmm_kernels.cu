@@ -1,53 +1,29 @@
-// pairhmm_kernels.cu -- instantiations of the forward kernels, their dispatch
-// table, and the arithmetic-peak microbenchmarks used as roofline
-// denominators.
+// pairhmm_kernels.cu -- dispatch to the forward-kernel instantiations
+// (kernels_r*.cu, kernels_multi.cu) and the arithmetic-peak microbenchmarks
+// used as roofline denominators.
 #include <cuda_runtime.h>
 
 #include "kernels.h"
-#include "pairhmm_fwd.cuh"
+#include "layout.h"
 
 namespace rodv {
 
-namespace {
+template <int R, bool MU>
+KernelInfo info_for(Precision prec, bool uniform, bool same, int variant);
 
-template <class P, int R, bool U, bool MU>
-KernelInfo info_of() {
-  KernelInfo k;
-  k.fn = reinterpret_cast<const void*>(&forward_kernel<P, R, U, MU>);
-  k.threads = Forward<P, R, U, MU>::kWarpsPerBlock * kWarp;
-  k.warps_per_block = Forward<P, R, U, MU>::kWarpsPerBlock;
-  k.smem_bytes = Forward<P, R, U, MU>::kWarpsPerBlock * TableShape<P, R>::kBytesPerWarp;
-  k.rows_per_lane = R;
-  k.multi = MU;
-  return k;
-}
-
-template <class P, bool U>
-KernelInfo single_pass(int R) {
-  switch (R) {
-    case 1: return info_of<P, 1, U, false>();
-    case 2: return info_of<P, 2, U, false>();
-    case 3: return info_of<P, 3, U, false>();
-    case 4: return info_of<P, 4, U, false>();
-    case 5: return info_of<P, 5, U, false>();
-    case 6: return info_of<P, 6, U, false>();
-    case 7: return info_of<P, 7, U, false>();
-    default: return info_of<P, 8, U, false>();
+KernelInfo forward_kernel_info(Precision prec, int rows_per_lane, bool uniform, bool multi,
+                               bool same, int variant) {
+  if (multi) return info_for<kMaxRowsPerLane, true>(prec, uniform, same, variant);
+  switch (rows_per_lane) {
+    case 1: return info_for<1, false>(prec, uniform, same, variant);
+    case 2: return info_for<2, false>(prec, uniform, same, variant);
+    case 3: return info_for<3, false>(prec, uniform, same, variant);
+    case 4: return info_for<4, false>(prec, uniform, same, variant);
+    case 5: return info_for<5, false>(prec, uniform, same, variant);
+    case 6: return info_for<6, false>(prec, uniform, same, variant);
+    case 7: return info_for<7, false>(prec, uniform, same, variant);
+    default: return info_for<8, false>(prec, uniform, same, variant);
   }
-}
-
-}  // namespace
-
-KernelInfo forward_kernel_info(Precision prec, int rows_per_lane, bool uniform, bool multi) {
-  if (prec == Precision::kF32x2) {
-    if (multi) return uniform ? info_of<F32x2, kMaxRowsPerLane, true, true>()
-                              : info_of<F32x2, kMaxRowsPerLane, false, true>();
-    return uniform ? single_pass<F32x2, true>(rows_per_lane)
-                   : single_pass<F32x2, false>(rows_per_lane);
-  }
-  if (multi) return uniform ? info_of<F64, kMaxRowsPerLane, true, true>()
-                            : info_of<F64, kMaxRowsPerLane, false, true>();
-  return uniform ? single_pass<F64, true>(rows_per_lane) : single_pass<F64, false>(rows_per_lane);
 }
 
 // ---- arithmetic-peak microbenchmarks (measurement only) -------------------

@@ -236,3 +236,23 @@ def test_invalid_inputs_fail_loudly(engine):
 def test_peaks_are_measured(engine):
     p = engine.measure_peaks()
     assert p["fp32_gflops"] > 1e4 and p["fp64_gflops"] > 1e3 and p["sm_mhz"] > 300
+
+
+def test_autotune_picks_variants_and_keeps_results(tmp_path):
+    """The autotuner picks one occupancy variant per work class, caches it, and
+    the results do not depend on the variant."""
+    from rodv_b200 import Engine
+    b = workloads.make_workload("uneven", scale=0.003)
+    e = Engine(0)
+    before = e.batch(b)
+    cache = str(tmp_path / "tune.txt")
+    variants = e.autotune(cache)
+    assert len(variants) == 18 and all(0 <= v < 4 for v in variants)
+    assert open(cache).read().count("\n") == 18
+    after = e.batch(b)
+    assert np.abs(after - before).max() < TOL
+    assert np.abs(after - oracle.batch_log10(b)).max() < TOL
+    e2 = Engine(0, autotune=1, tune_cache=cache)   # loads the cache, no re-tuning
+    assert np.abs(e2.batch(b) - before).max() < TOL
+    e.close()
+    e2.close()
