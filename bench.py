@@ -144,8 +144,8 @@ def sized_sample(name: str, seed: int, seconds: float, threads: int):
 def sample_for_cpu(name: str, seed: int, target_cells: float):
     """A seeded prefix of the workload holding about target_cells cells."""
     from rodv_b200 import workloads
-    full_regions = {"uneven": 10_000, "stream": 1_000, "long": 2_000, "underflow": 200_000,
-                    "plain": 1, "tiny": 8}[name]
+    full_regions = {"uneven": 10_000, "uneven_windows": 10_000, "stream": 1_000, "long": 2_000,
+                    "underflow": 200_000, "plain": 1, "tiny": 8}[name]
     probe = workloads.make_workload(name, seed=seed, scale=min(1.0, 50 / full_regions))
     per_region = probe.cells() / max(1, probe.num_regions)
     n = max(1, min(full_regions, int(target_cells / per_region)))
@@ -271,6 +271,8 @@ def run_engine(args, world, rank, local):
     line = None
     if rank == 0:
         fp32_avg_s = sum(fp32_ms) / len(fp32_ms) / 1e3
+        if fp32_avg_s <= 0:
+            raise RuntimeError("the FP32 pass was not timed (fp32_ms = 0)")
         achieved = FLOPS_PER_CELL * cells / fp32_avg_s / 1e12
         peak = peaks["fp32_gflops"] / 1e3
         plain = plain_form(eng, args) if args.plain_pairs > 0 else None

@@ -209,7 +209,8 @@ rodv_status rodv_autotune(rodv_engine* engine, const char* cache_path, int32_t f
 /* Human-readable name of a status code (static storage). */
 const char* rodv_status_string(rodv_status status);
 
-/* Details of the last failure on this engine (static until the next call). */
+/* Details of the last failure on this engine (static until the next call);
+ * with engine == NULL, of the last failed rodv_engine_create. */
 const char* rodv_last_error(rodv_engine* engine);
 
 #ifdef __cplusplus

@@ -100,7 +100,8 @@ class Engine:
         h = ctypes.c_void_p()
         st = self.lib.rodv_engine_create(ctypes.byref(opts), ctypes.byref(h))
         if st != _lib.RODV_OK:
-            raise RodvError(st, "engine creation failed")
+            detail = self.lib.rodv_last_error(None) or b""
+            raise RodvError(st, "engine creation failed: " + detail.decode(errors="replace"))
         self.h = h
         self.device = device
 

@@ -2,6 +2,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <string>
 
 #include "engine.h"
 
@@ -23,6 +24,10 @@ void rodv_default_options(rodv_options* opts) {
   opts->tune_cache = nullptr;
 }
 
+// Message of the last failed rodv_engine_create (rodv_last_error(NULL)).
+static std::mutex g_create_mu;
+static std::string g_create_error;
+
 rodv_status rodv_engine_create(const rodv_options* opts, rodv_engine** out) {
   if (!out) return RODV_ERR_INVALID_ARG;
   *out = nullptr;
@@ -33,6 +38,10 @@ rodv_status rodv_engine_create(const rodv_options* opts, rodv_engine** out) {
   if (!e) return RODV_ERR_OUT_OF_MEMORY;
   rodv_status s = e->init();
   if (s != RODV_OK) {
+    {
+      std::lock_guard<std::mutex> lk(g_create_mu);
+      g_create_error = e->last_error();
+    }
     delete e;
     return s;
   }
@@ -168,7 +177,10 @@ const char* rodv_status_string(rodv_status s) {
 }
 
 const char* rodv_last_error(rodv_engine* engine) {
-  if (!engine) return "";
+  if (!engine) {
+    std::lock_guard<std::mutex> lk(g_create_mu);
+    return g_create_error.c_str();
+  }
   return engine->impl->last_error();
 }
 

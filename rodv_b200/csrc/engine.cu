@@ -162,6 +162,7 @@ rodv_status Engine::cuda_fail(cudaError_t e, const char* where) {
   } while (0)
 
 rodv_status Engine::init() {
+  cudaGetLastError();  // clear a stale error of an earlier call on this thread
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
     return fail(RODV_ERR_NO_DEVICE, "no CUDA device visible");
@@ -183,9 +184,10 @@ rodv_status Engine::init() {
   RODV_CUDA(tables_.ensure(bytes));
   uint8_t* base = static_cast<uint8_t*>(tables_.ptr);
   size_t o = 0;
+  cudaError_t ce = cudaSuccess;
   auto put = [&](const void* src, size_t n) -> void* {
     void* dst = base + o;
-    cudaMemcpy(dst, src, n, cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess) ce = cudaMemcpy(dst, src, n, cudaMemcpyHostToDevice);
     o = align_up(o + n);
     return dst;
   };
@@ -193,7 +195,7 @@ rodv_status Engine::init() {
   tab_.mm_f = static_cast<const float*>(put(t.mm_f.data(), kMmTableSize * 4));
   tab_.ph2pr_d = static_cast<const double*>(put(t.ph2pr_d.data(), 128 * 8));
   tab_.mm_d = static_cast<const double*>(put(t.mm_d.data(), kMmTableSize * 8));
-  RODV_CUDA(cudaGetLastError());
+  RODV_CUDA(ce);
   ready_ = true;
   if (opt_.tune_cache && opt_.tune_cache[0]) load_tuning(opt_.tune_cache);
   if (opt_.autotune) {
@@ -342,6 +344,10 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
     plan.off_lists[c] = o;
     o = align_up(o + (size_t)plan.pairs[c] * sizeof(PairRef));
   }
+  // forced FP64: the lists are full from the start; their lengths are uploaded
+  // too and copied into the counters at every run
+  plan.off_preset = o;
+  if (fp64) o = align_up(o + kNumClasses * 4);
   // FP32 runs fill the lists on the device; only forced-FP64 lists are uploaded.
   plan.upload_bytes = fp64 ? o : lists_begin;
   plan.off_out = o; o = align_up(o + pairs * 8);
@@ -414,6 +420,10 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
     return fail(RODV_ERR_INVALID_BASE, msg);
   }
 
+  if (fp64) {
+    uint32_t* preset = reinterpret_cast<uint32_t*>(s + plan.off_preset);
+    for (int c = 0; c < kNumClasses; ++c) preset[c] = plan.pairs[c];
+  }
   // ---- work: same-haplotype items, leftovers, forced-FP64 lists ----
   std::vector<uint64_t> region_out(G);
   for (uint32_t g = 0, acc = 0; g < G; ++g) {
@@ -508,19 +518,17 @@ rodv_status Engine::launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, in
 }
 
 rodv_status Engine::launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stats* st,
-                               bool timed) {
+                               bool timed, bool split, int parts) {
   ArenaView a = arena_view(plan, dbase, tab_);
-  RODV_CUDA(cudaMemsetAsync(a.counts, 0, kCountWords * 4, stream_));
-  if (plan.fp64) {
-    // every pair goes to the FP64 kernels: the uploaded lists are full
-    std::vector<uint32_t> preset(kNumClasses);
-    for (int c = 0; c < kNumClasses; ++c) preset[c] = plan.pairs[c];
-    RODV_CUDA(cudaMemcpyAsync(a.counts + kCtrRescue, preset.data(), kNumClasses * 4,
-                              cudaMemcpyHostToDevice, stream_));
-  }
   uint32_t launches = 0;
+  if (parts & 1) {
+    RODV_CUDA(cudaMemsetAsync(a.counts, 0, kCountWords * 4, stream_));
+    if (plan.fp64)  // every pair goes to the FP64 kernels: the uploaded lists are full
+      RODV_CUDA(cudaMemcpyAsync(a.counts + kCtrRescue, dbase + plan.off_preset,
+                                kNumClasses * 4, cudaMemcpyDeviceToDevice, stream_));
+  }
   if (timed) RODV_CUDA(cudaEventRecord(ev_[0], stream_));
-  if (!plan.fp64) {
+  if (!plan.fp64 && (parts & 1)) {
     for (int c = 0; c < kNumClasses; ++c) {
       for (int same = 1; same >= 0; --same) {
         if (!(same ? plan.same_items[c] : plan.diff_items[c])) continue;
@@ -530,8 +538,8 @@ rodv_status Engine::launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stat
       }
     }
   }
-  if (timed) RODV_CUDA(cudaEventRecord(ev_[1], stream_));
-  for (int c = 0; c < kNumClasses; ++c) {
+  if (timed || split) RODV_CUDA(cudaEventRecord(ev_[1], stream_));
+  for (int c = 0; c < kNumClasses && (parts & 2); ++c) {
     if (!plan.pairs[c]) continue;
     const KernelInfo k =
         forward_kernel_info(Precision::kF64, class_rows(c), class_uniform(c), class_multi(c));
@@ -583,7 +591,7 @@ rodv_status Engine::run_host(const rodv_batch& b, double* out, rodv_stats* st, b
   uint8_t* d = static_cast<uint8_t*>(arena_.ptr);
   RODV_CUDA(cudaEventRecord(ev_[3], stream_));
   RODV_CUDA(cudaMemcpyAsync(d, staging_.ptr, plan.upload_bytes, cudaMemcpyHostToDevice, stream_));
-  s = launch_all(plan, d, st, true);
+  s = launch_all(plan, d, st, true, true, 3);
   if (s != RODV_OK) return s;
   uint8_t* hs = static_cast<uint8_t*>(out_staging_.ptr);
   RODV_CUDA(cudaMemcpyAsync(hs, d + plan.off_out, plan.num_pairs * 8, cudaMemcpyDeviceToHost,
@@ -638,13 +646,38 @@ rodv_status Engine::run_device(rodv_device_batch* db, rodv_stats* st) {
   RODV_CUDA(cudaSetDevice(device_));
   uint8_t* d = static_cast<uint8_t*>(db->arena.ptr);
   const auto t0 = std::chrono::steady_clock::now();
-  rodv_status s = launch_all(db->plan, d, st, true);
-  if (s != RODV_OK) return s;
+  if (!db->graph[0]) {
+    // Capture once, as two graphs (FP32 part: counter reset and the FP32 class
+    // launches; FP64 part: the rescue launches) so that an event between them
+    // times the FP32 pass; later runs are two graph launches.
+    for (int part = 0; part < 2; ++part) {
+      rodv_stats cap{};
+      RODV_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+      rodv_status s = launch_all(db->plan, d, &cap, false, false, part == 0 ? 1 : 2);
+      cudaGraph_t g = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(stream_, &g);
+      if (s != RODV_OK) {
+        if (g) cudaGraphDestroy(g);
+        return s;
+      }
+      if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+      const cudaError_t ie = cudaGraphInstantiate(&db->graph[part], g, 0);
+      cudaGraphDestroy(g);
+      if (ie != cudaSuccess) return cuda_fail(ie, "cudaGraphInstantiate");
+      db->graph_launches += cap.kernel_launches;
+    }
+  }
+  RODV_CUDA(cudaEventRecord(ev_[0], stream_));
+  RODV_CUDA(cudaGraphLaunch(db->graph[0], stream_));
+  RODV_CUDA(cudaEventRecord(ev_[1], stream_));
+  RODV_CUDA(cudaGraphLaunch(db->graph[1], stream_));
+  RODV_CUDA(cudaEventRecord(ev_[2], stream_));
   RODV_CUDA(cudaStreamSynchronize(stream_));
   uint32_t counts[kCountWords];
   RODV_CUDA(cudaMemcpy(counts, d + db->plan.off_counts, sizeof(counts), cudaMemcpyDeviceToHost));
   if (st) {
     fill_stats(st, db->plan, counts);
+    st->kernel_launches += db->graph_launches;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ev_[0], ev_[2]);
     st->device_ms = ms;
@@ -748,7 +781,8 @@ rodv_status Engine::plain(rodv_device_batch* db, double* out, rodv_stats* st) {
 // Autotuning: per work class, the occupancy variant (register budget) of the
 // same-haplotype FP32 kernel, chosen by timing every variant on a synthetic
 // batch of that class (reads of 32R-5 bases, or 700 for multi-pass, against
-// 400- or 1,200-base haplotypes).  Results are cached per device.
+// 400- or 1,200-base haplotypes; ~16 items per resident warp).  Results are
+// cached per device.
 // ---------------------------------------------------------------------------
 std::string Engine::device_key() const {
   std::string k = device_name_;
@@ -798,9 +832,13 @@ rodv_status Engine::autotune(const char* cache_path, int force, int32_t* variant
     const bool multi = class_multi(c), uni = class_uniform(c);
     const uint32_t L = multi ? 700 : (uint32_t)std::max(1, 32 * R - 5);
     const uint32_t H = multi ? 1200 : 400;
+    // Enough items that every warp of the largest grid takes ~16 of them
+    // (4 for multi-pass), so the timing reflects per-item throughput and not
+    // the tail of the work queue.
+    const uint64_t max_warps = (uint64_t)num_sms_ * kVariantMinBlocks[kTuneVariants - 1] * 4;
+    const uint64_t items = max_warps * (multi ? 4 : 16);
     const int regions = 16, haps = 4;
-    const int reads = (int)std::max<uint64_t>(2, std::min<uint64_t>(512, 1500000000ull /
-                                                                        ((uint64_t)regions * haps * L * H)));
+    const int reads = (int)std::max<uint64_t>(2, 2 * items / (regions * haps) + 1);
     std::vector<uint8_t> hb, rb, q, ins, del, gcp;
     std::vector<uint64_t> ho, ro;
     std::vector<uint32_t> hl, rl;

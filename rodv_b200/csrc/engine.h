@@ -72,6 +72,7 @@ struct PackedPlan {
   size_t off_same[kNumClasses] = {};
   size_t off_diff[kNumClasses] = {};
   size_t off_lists[kNumClasses] = {};      // FP64 work lists (rescued or forced)
+  size_t off_preset = 0;                   // forced FP64: list lengths (uploaded)
   size_t upload_bytes = 0;                 // the H2D part starts at 0
   size_t off_out = 0, off_counts = 0, off_scratch = 0;
   size_t total_bytes = 0;
@@ -103,7 +104,8 @@ class Engine {
 
  private:
   rodv_status pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64);
-  rodv_status launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stats* st, bool timed);
+  rodv_status launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stats* st, bool timed,
+                         bool split, int parts);
   rodv_status launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, int cls, bool same,
                                 int variant, int blocks_cap);
   rodv_status check_errors(const PackedPlan& plan, uint8_t* dbase);
@@ -141,4 +143,12 @@ struct rodv_engine {
 struct rodv_device_batch {
   rodv::PackedPlan plan;
   rodv::DeviceMem arena;
+  // The per-step launch sequence (counter reset, FP32 and FP64 class
+  // launches) captured once as two CUDA graphs and replayed by every run.
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // FP32 part, FP64 part
+  uint32_t graph_launches = 0;
+  ~rodv_device_batch() {
+    for (cudaGraphExec_t g : graph)
+      if (g) cudaGraphExecDestroy(g);
+  }
 };

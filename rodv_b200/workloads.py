@@ -4,7 +4,14 @@ The reference publishes no benchmark dataset; these generators produce
 seeded stand-ins with the stated shapes, sizes and value distributions:
 
 * ``plain``      1 region, 8 haps of 250-400 bp, 64 reads of 150 bp
-* ``uneven``     10,000 regions, 20-200 reads (50-250 bp) x 2-16 haps (100-600 bp)
+* ``uneven``     10,000 regions, 20-200 reads (50-250 bp) x 2-16 haps (100-600 bp);
+                 a region's haplotypes are mutated copies of one locus whose
+                 length is drawn per region (assembled haplotypes of one
+                 active region, as in the reference's resouces/pairhmm_debug.txt)
+* ``uneven_windows``  the same shape with each haplotype a random window of
+                 its own length (the reference unit-test generator's model):
+                 reads from one haplotype's flank do not align to another, so
+                 ~27% of pairs fall below the FP32 threshold (FP64 stress)
 * ``long``       2,000 pairs, reads 1,000-2,000 bp vs haps 2,000-5,000 bp
 * ``underflow``  200,000 pairs, 250 bp reads vs unrelated random 400 bp haps,
                  base quals Phred 2-8
@@ -13,7 +20,8 @@ seeded stand-ins with the stated shapes, sizes and value distributions:
 Within a region the haplotypes are mutated copies of one uniform-ACGT base
 sequence and reads are mutated substrings of a uniformly chosen haplotype,
 the model of the reference's own generator
-(src/core/test/pairhmm_schedule_unittest.cpp:244-334).  Mutation model:
+(src/core/test/pairhmm_schedule_unittest.cpp:244-334); ``uneven`` and
+``stream`` copy the whole locus, the others take random windows.  Mutation model:
 1% substitutions and 0.1% indels of 1-3 bp per base (5% / 1% for ``long``).
 Base quals are uniform Phred 10-40 unless stated; ins = del = 45, gcp = 10.
 """
@@ -28,7 +36,7 @@ from .batch import Batch, REGION_DTYPE
 ACGT = np.frombuffer(b"ACGT", dtype=np.uint8)
 
 SEEDS: Dict[str, int] = {"plain": 1001, "uneven": 1002, "long": 1003, "underflow": 1004,
-                         "stream": 1005, "tiny": 1006}
+                         "stream": 1005, "tiny": 1006, "uneven_windows": 1007}
 
 
 def _random_seq(rng: np.random.Generator, n: int) -> np.ndarray:
@@ -86,11 +94,21 @@ class _Builder:
 
 
 def _region(rng, n_haps, hap_len_rng, n_reads, read_len_rng, p_sub, p_indel, bq=(10, 40),
-            ins=45, dele=45, gcp=10, independent_haps=False):
-    hap_lens = rng.integers(hap_len_rng[0], hap_len_rng[1] + 1, size=n_haps)
-    base = _random_seq(rng, int(hap_lens.max()) + 16)
-    haps = []
-    for hl in hap_lens:
+            ins=45, dele=45, gcp=10, independent_haps=False, locus=False):
+    """One region.  Haplotypes are mutated copies of one base sequence: random
+    windows of it with their own lengths (the reference generator's model), or,
+    with ``locus``, full copies of one locus whose length is drawn per region."""
+    if locus:
+        loc_len = int(rng.integers(hap_len_rng[0], hap_len_rng[1] + 1))
+        base = _random_seq(rng, loc_len)
+        haps = [_mutate(rng, base, p_sub, p_indel) for _ in range(n_haps)]
+        haps = [h if len(h) else base.copy() for h in haps]
+        hap_lens = None
+    else:
+        hap_lens = rng.integers(hap_len_rng[0], hap_len_rng[1] + 1, size=n_haps)
+        base = _random_seq(rng, int(hap_lens.max()) + 16)
+        haps = []
+    for hl in (hap_lens if hap_lens is not None else []):
         if independent_haps:
             haps.append(_random_seq(rng, int(hl)))
             continue
@@ -122,16 +140,17 @@ def make_workload(name: str, seed: int | None = None, scale: float = 1.0) -> Bat
     if name == "plain":
         haps, reads, quals = _region(rng, 8, (250, 400), 64, (150, 150), 0.01, 0.001)
         b.add_region(haps, reads, quals)
-    elif name == "uneven":
+    elif name in ("uneven", "uneven_windows"):
         for _ in range(max(1, int(round(10_000 * scale)))):
             nh = int(rng.integers(2, 17))
             nr = int(rng.integers(20, 201))
-            b.add_region(*_region(rng, nh, (100, 600), nr, (50, 250), 0.01, 0.001))
+            b.add_region(*_region(rng, nh, (100, 600), nr, (50, 250), 0.01, 0.001,
+                                  locus=(name == "uneven")))
     elif name == "stream":
         for _ in range(max(1, int(round(1_000 * scale)))):
             nh = int(rng.integers(1, 33))
             nr = int(rng.integers(1, 301))
-            b.add_region(*_region(rng, nh, (100, 800), nr, (50, 250), 0.01, 0.001))
+            b.add_region(*_region(rng, nh, (100, 800), nr, (50, 250), 0.01, 0.001, locus=True))
     elif name == "long":
         for _ in range(max(1, int(round(2_000 * scale)))):
             b.add_region(*_region(rng, 1, (2000, 5000), 1, (1000, 2000), 0.05, 0.01))

@@ -256,3 +256,21 @@ def test_autotune_picks_variants_and_keeps_results(tmp_path):
     assert np.abs(e2.batch(b) - before).max() < TOL
     e.close()
     e2.close()
+
+
+def test_forced_fp64_device_batch_graph_replays():
+    """A device batch of an FP64-forced engine: the captured launch graph
+    replays with the list lengths restored from device memory every run."""
+    from rodv_b200 import Engine
+    e = Engine(0, force_fp64=True)
+    b = workloads.make_workload("tiny", scale=1.0)
+    db = e.upload(b)
+    s1 = db.run()
+    r1 = db.download()
+    s2 = db.run()
+    r2 = db.download()
+    assert s1["fp64_pairs"] == s2["fp64_pairs"] == b.num_pairs
+    assert np.array_equal(r1, r2)
+    assert np.abs(r1 - oracle.batch_log10(b, oracle.FP64)).max() < 1e-9
+    db.free()
+    e.close()
