@@ -6,16 +6,18 @@
 //   1. validate and pack on the host (threads over regions and reads) into one
 //      pinned staging buffer laid out exactly like the device arena;
 //   2. one H2D copy of the staging buffer;
-//   3. per work class, one persistent FP32 launch over its same-haplotype
-//      items (two reads of a region against one haplotype per warp) and one
-//      over the leftover two-haplotype items; pairs whose scaled FP32 result
-//      is below 1e-28 are appended to the class's FP64 list on the device;
+//   3. per work class, one persistent FP32 launch over its chain items (two
+//      reads of a region against all its haplotypes per warp; reads of up to
+//      256 bases) or, for longer reads, over same-haplotype items (two reads
+//      against one haplotype) and leftover two-haplotype items; pairs whose
+//      scaled FP32 result is below 1e-28 are appended to the class's FP64
+//      list on the device;
 //   4. per work class, one persistent FP64 launch that drains that list (its
 //      length is read by the kernel, never by the host);
 //   5. one D2H copy of the log10 results.
 // The reference instead groups pairs into SIMD-width groups by padded area
 // (greedy_grouping, :46-105) and sends leftovers to a per-pair kernel; here
-// work classes (rows per lane) and same-haplotype pairing play that part.
+// work classes (rows per lane) and per-region chains play that part.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -99,8 +101,8 @@ ArenaView arena_view(const PackedPlan& p, uint8_t* base, const PriorTables& tab)
 // measured best for each rows-per-lane value on B200.
 int default_variant(int cls) {
   const int R = class_rows(cls);
-  if (class_multi(cls) || R >= 7) return 0;  // 4 blocks/SM: up to 128 registers
-  if (R >= 4) return 2;                      // 6 blocks/SM: up to 80 registers
+  if (class_multi(cls) || R >= 3) return 0;  // 4 blocks/SM: up to 128 registers
+  if (R == 2) return 2;                      // 6 blocks/SM: up to 80 registers
   return 3;                                  // 8 blocks/SM: up to 64 registers
 }
 
@@ -196,6 +198,19 @@ rodv_status Engine::init() {
   tab_.ph2pr_d = static_cast<const double*>(put(t.ph2pr_d.data(), 128 * 8));
   tab_.mm_d = static_cast<const double*>(put(t.mm_d.data(), kMmTableSize * 8));
   RODV_CUDA(ce);
+  // Kernels whose tables exceed the default 48 KB of dynamic shared memory
+  // per block opt in to their size.
+  for (int c = 0; c < kNumClasses; ++c)
+    for (int p = 0; p < 3; ++p)
+      for (int v = 0; v < kTuneVariants; ++v) {
+        const Precision pr = p == 2 ? Precision::kF64 : Precision::kF32x2;
+        if (v > 0 && forward_kernel_variants(pr, p == 0) == 1) continue;
+        const KernelInfo k =
+            forward_kernel_info(pr, class_rows(c), class_uniform(c), class_multi(c), p == 0, v);
+        if (k.fn && k.smem_bytes > 48 * 1024)
+          RODV_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         k.smem_bytes));
+      }
   ready_ = true;
   if (opt_.tune_cache && opt_.tune_cache[0]) load_tuning(opt_.tune_cache);
   if (opt_.autotune) {
@@ -241,19 +256,20 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   plan.num_reads = b.num_reads;
   plan.regions.assign(b.regions, b.regions + G);
 
-  // haplotype code buffer: [pad][hap 0][pad][hap 1]...[hap n-1][pad + max len + pad]
+  // haplotype code buffer: [pad][hap 0][sep][hap 1][sep]...[hap n-1][sep]
+  // [pad + max len + pad]; any run of consecutive haplotypes is one chain.
   std::vector<uint64_t> hap_code_off(b.num_haps);
-  uint64_t hb = 0;
+  uint64_t hb = kHapPad;
   uint32_t max_h = 0;
   for (uint32_t h = 0; h < b.num_haps; ++h) {
     const uint32_t len = b.hap_lengths[h];
     if (len == 0) return fail(RODV_ERR_INVALID_ARG, "haplotype " + std::to_string(h) + " is empty");
     if (len > RODV_MAX_HAP_LEN) return fail(RODV_ERR_TOO_LONG, "haplotype longer than limit");
-    hb += kHapPad;
     hap_code_off[h] = hb;
-    hb += len;
+    hb += len + 1;
     max_h = std::max(max_h, len);
   }
+  const uint64_t tail_begin = hb;
   hb += kHapPad + max_h + kHapPad;
   plan.hap_code_bytes = hb;
   plan.max_hap_len = max_h;
@@ -288,39 +304,111 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
     }
   });
 
-  // ---- per region and class: reads, same items, leftovers, pairs ----
-  std::vector<uint32_t> rc((size_t)G * kNumClasses, 0);   // reads of class c in region g
-  parallel_for(G, 256, [&](size_t lo, size_t hi) {
+  // ---- per region and class: reads, chain items, same items, leftovers ----
+  // Single-pass reads of a region are sorted by (uniform gaps, length) and
+  // paired neighbour by neighbour; a pair's class is that of its longer read
+  // (uniform only if both are), an odd last read forms a one-read chain.
+  // Each pair takes ceil(haps / chain_haps[class]) chain items.  Multi-pass reads
+  // keep their own class: same-haplotype items per haplotype, leftovers in
+  // two-haplotype items.
+  const uint32_t K = kNumClasses;
+  auto sorted_single = [&](const rodv_region& rg, std::vector<uint32_t>& out_reads) {
+    out_reads.clear();
+    for (uint32_t r = 0; r < rg.num_reads; ++r) {
+      const uint32_t read = rg.read_start + r;
+      if (!class_multi(read_class[read])) out_reads.push_back(read);
+    }
+    std::stable_sort(out_reads.begin(), out_reads.end(), [&](uint32_t x, uint32_t y) {
+      const uint32_t kx = ((read_class[x] & 1u) << 20) | b.read_lengths[x];
+      const uint32_t ky = ((read_class[y] & 1u) << 20) | b.read_lengths[y];
+      return kx < ky;
+    });
+  };
+  auto pair_class = [&](uint32_t x, uint32_t y) {
+    const uint32_t len = std::max(b.read_lengths[x], b.read_lengths[y]);
+    return class_of(len, (read_class[x] & 1) && (read_class[y] & 1));
+  };
+  std::vector<uint32_t> rc((size_t)G * K, 0);      // reads of class c in region g
+  std::vector<uint32_t> rpairs((size_t)G * K, 0);  // read pairs (or single reads) of chain class c
+  std::vector<uint32_t> chains((size_t)G * K, 0);  // chain items of class c in region g
+  std::vector<uint64_t> cpairs((size_t)G * K, 0);  // pairs those chains compute
+  std::vector<uint64_t> hsum(G, 0);
+  parallel_for(G, 64, [&](size_t lo, size_t hi) {
+    std::vector<uint32_t> sr;
     for (size_t g = lo; g < hi; ++g) {
       const rodv_region& rg = b.regions[g];
-      for (uint32_t r = 0; r < rg.num_reads; ++r) rc[g * kNumClasses + read_class[rg.read_start + r]]++;
+      for (uint32_t r = 0; r < rg.num_reads; ++r) rc[g * K + read_class[rg.read_start + r]]++;
+      for (uint32_t h = 0; h < rg.num_haps; ++h) hsum[g] += b.hap_lengths[rg.hap_start + h];
+      if (fp64) continue;
+      sorted_single(rg, sr);
+      for (size_t k = 0; k < sr.size(); k += 2) {
+        const bool two = k + 1 < sr.size();
+        const int c = two ? pair_class(sr[k], sr[k + 1]) : read_class[sr[k]];
+        rpairs[g * K + c] += 1;
+        cpairs[g * K + c] += (uint64_t)rg.num_haps * (two ? 2 : 1);
+      }
     }
   });
-  // prefix offsets (within each class) of same items, leftovers, FP64 list entries
-  std::vector<uint64_t> same_off((size_t)G * kNumClasses), left_off((size_t)G * kNumClasses),
-      list_off((size_t)G * kNumClasses);
-  uint64_t same_tot[kNumClasses] = {}, left_tot[kNumClasses] = {}, list_tot[kNumClasses] = {};
-  for (uint32_t g = 0; g < G; ++g) {
+  // Haplotypes per chain item, per class: the longest chains (up to
+  // kChainHaps) that still leave every resident warp of the class's launch
+  // several items; a small batch gets short chains (down to one haplotype).
+  const uint64_t target_items = (uint64_t)num_sms_ * 16 * 4;
+  for (int c = 0; c < kSinglePassClasses; ++c) {
+    plan.chain_haps[c] = 1;
+    for (uint32_t cap = kChainHaps; cap >= 1; cap /= 2) {
+      uint64_t items = 0;
+      for (uint32_t g = 0; g < G; ++g)
+        items += (uint64_t)rpairs[(size_t)g * K + c] * ((b.regions[g].num_haps + cap - 1) / cap);
+      if (items >= target_items || cap == 1) {
+        plan.chain_haps[c] = cap;
+        break;
+      }
+    }
+  }
+  for (uint32_t g = 0; g < G; ++g)
+    for (int c = 0; c < kSinglePassClasses; ++c)
+      chains[(size_t)g * K + c] = rpairs[(size_t)g * K + c] *
+          ((b.regions[g].num_haps + plan.chain_haps[c] - 1) / plan.chain_haps[c]);
+  // Chain items are laid out region by region in decreasing order of the
+  // region's haplotype-length sum (a chain's cost), so the persistent
+  // kernels take the longest chains first.
+  std::vector<uint32_t> order(G);
+  for (uint32_t g = 0; g < G; ++g) order[g] = g;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](uint32_t x, uint32_t y) { return hsum[x] > hsum[y]; });
+  // prefix offsets (within each class) of same/chain items, leftovers, FP64 list entries
+  std::vector<uint64_t> same_off((size_t)G * K), left_off((size_t)G * K), list_off((size_t)G * K);
+  uint64_t same_tot[kNumClasses] = {}, left_tot[kNumClasses] = {}, list_tot[kNumClasses] = {},
+           cap_tot[kNumClasses] = {};
+  for (uint32_t i = 0; i < G; ++i) {
+    const uint32_t g = order[i];
     const uint64_t H = b.regions[g].num_haps;
     for (int c = 0; c < kNumClasses; ++c) {
-      const uint64_t n = rc[(size_t)g * kNumClasses + c];
-      same_off[(size_t)g * kNumClasses + c] = same_tot[c];
-      left_off[(size_t)g * kNumClasses + c] = left_tot[c];
-      list_off[(size_t)g * kNumClasses + c] = list_tot[c];
-      same_tot[c] += H * (n / 2);
-      left_tot[c] += H * (n & 1);
+      const uint64_t n = rc[(size_t)g * K + c];
+      same_off[(size_t)g * K + c] = same_tot[c];
+      left_off[(size_t)g * K + c] = left_tot[c];
+      list_off[(size_t)g * K + c] = list_tot[c];
       list_tot[c] += H * n;
+      if (class_multi(c)) {
+        same_tot[c] += H * (n / 2);
+        left_tot[c] += H * (n & 1);
+        cap_tot[c] += H * n;
+      } else {
+        same_tot[c] += chains[(size_t)g * K + c];
+        cap_tot[c] += cpairs[(size_t)g * K + c];
+      }
     }
   }
   for (int c = 0; c < kNumClasses; ++c) {
-    plan.pairs[c] = (uint32_t)list_tot[c];
+    // FP64 list capacity: every pair whose FP32 work is in class c (or, FP64
+    // forced, every pair whose read is of class c)
+    plan.pairs[c] = (uint32_t)(fp64 ? list_tot[c] : cap_tot[c]);
     plan.same_items[c] = fp64 ? 0u : (uint32_t)same_tot[c];
     plan.diff_items[c] = fp64 ? 0u : (uint32_t)((left_tot[c] + 1) / 2);
   }
   for (uint32_t g = 0; g < G; ++g) {
     const rodv_region& rg = b.regions[g];
-    if (rc[(size_t)g * kNumClasses + kSinglePassClasses] ||
-        rc[(size_t)g * kNumClasses + kSinglePassClasses + 1])
+    if (rc[(size_t)g * K + kSinglePassClasses] || rc[(size_t)g * K + kSinglePassClasses + 1])
       for (uint32_t h = 0; h < rg.num_haps; ++h)
         plan.multi_max_hap = std::max(plan.multi_max_hap, b.hap_lengths[rg.hap_start + h]);
   }
@@ -333,7 +421,8 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   plan.off_reads = o; o = align_up(o + (size_t)b.num_reads * sizeof(ReadDesc));
   for (int c = 0; c < kNumClasses; ++c) {
     plan.off_same[c] = o;
-    o = align_up(o + (size_t)plan.same_items[c] * sizeof(SameItem));
+    const size_t item = class_multi(c) ? sizeof(SameItem) : sizeof(ChainItem);
+    o = align_up(o + (size_t)plan.same_items[c] * item);
   }
   for (int c = 0; c < kNumClasses; ++c) {
     plan.off_diff[c] = o;
@@ -382,18 +471,19 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       const uint8_t* src = b.hap_bases + b.hap_offsets[h];
       uint8_t* dst = codes + hap_code_off[h];
       const uint32_t n = b.hap_lengths[h];
-      std::memset(dst - kHapPad, 0, kHapPad);
       for (uint32_t k = 0; k < n; ++k) {
         const uint8_t c = kCodes.v[src[k]];
         if (c == 0xff) bad_base.store((int)src[k]);
         dst[k] = c;
       }
+      dst[n] = kSep;
       hd[h].code_off = hap_code_off[h];
       hd[h].len = n;
       hd[h].pad_ = 0;
     }
   });
-  std::memset(codes + hb - (kHapPad + max_h + kHapPad), 0, kHapPad + max_h + kHapPad);
+  std::memset(codes, 0, kHapPad);
+  std::memset(codes + tail_begin, 0, hb - tail_begin);
   // ---- read rows ----
   uint32_t* rw = reinterpret_cast<uint32_t*>(s + plan.off_read_rows);
   ReadDesc* rdesc = reinterpret_cast<ReadDesc*>(s + plan.off_reads);
@@ -424,7 +514,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
     uint32_t* preset = reinterpret_cast<uint32_t*>(s + plan.off_preset);
     for (int c = 0; c < kNumClasses; ++c) preset[c] = plan.pairs[c];
   }
-  // ---- work: same-haplotype items, leftovers, forced-FP64 lists ----
+  // ---- work: chain items, same-haplotype items, leftovers, forced-FP64 lists ----
   std::vector<uint64_t> region_out(G);
   for (uint32_t g = 0, acc = 0; g < G; ++g) {
     region_out[g] = acc;
@@ -434,30 +524,46 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   for (int c = 0; c < kNumClasses; ++c) leftovers[c].resize(left_tot[c]);
   parallel_for(G, 64, [&](size_t lo, size_t hi) {
     std::vector<uint32_t> byclass[kNumClasses];
+    std::vector<uint32_t> sr;
     for (size_t g = lo; g < hi; ++g) {
       const rodv_region& rg = b.regions[g];
+      const uint32_t N = rg.num_reads;
+      // out index of (haplotype h of the region, read rr)
+      auto out_of = [&](uint32_t h, uint32_t rr) {
+        return (uint32_t)(region_out[g] + (uint64_t)h * N + (rr - rg.read_start));
+      };
+      if (!fp64) {
+        sorted_single(rg, sr);
+        uint64_t next[kNumClasses];
+        for (int c = 0; c < kNumClasses; ++c) next[c] = same_off[g * K + c];
+        for (size_t k = 0; k < sr.size(); k += 2) {
+          const bool two = k + 1 < sr.size();
+          const int c = two ? pair_class(sr[k], sr[k + 1]) : read_class[sr[k]];
+          ChainItem* ci = reinterpret_cast<ChainItem*>(s + plan.off_same[c]);
+          const uint32_t cap = plan.chain_haps[c];
+          for (uint32_t h0 = 0; h0 < rg.num_haps; h0 += cap)
+            ci[next[c]++] = ChainItem{rg.hap_start + h0, std::min(cap, rg.num_haps - h0), sr[k],
+                                      two ? sr[k + 1] : kNoPair, out_of(h0, sr[k]), N};
+        }
+      }
       for (auto& v : byclass) v.clear();
-      for (uint32_t r = 0; r < rg.num_reads; ++r)
-        byclass[read_class[rg.read_start + r]].push_back(rg.read_start + r);
+      for (uint32_t r = 0; r < N; ++r) byclass[read_class[rg.read_start + r]].push_back(rg.read_start + r);
       for (int c = 0; c < kNumClasses; ++c) {
         const std::vector<uint32_t>& rd = byclass[c];
-        if (rd.empty()) continue;
-        SameItem* si = reinterpret_cast<SameItem*>(s + plan.off_same[c]) +
-                       same_off[g * kNumClasses + c];
-        PairRef* lf = leftovers[c].data() + left_off[g * kNumClasses + c];
-        PairRef* li = reinterpret_cast<PairRef*>(s + plan.off_lists[c]) +
-                      list_off[g * kNumClasses + c];
+        if (rd.empty() || (!fp64 && !class_multi(c))) continue;
+        SameItem* si = reinterpret_cast<SameItem*>(s + plan.off_same[c]) + same_off[g * K + c];
+        PairRef* lf = leftovers[c].data() + left_off[g * K + c];
+        PairRef* li = reinterpret_cast<PairRef*>(s + plan.off_lists[c]) + list_off[g * K + c];
         for (uint32_t h = 0; h < rg.num_haps; ++h) {
           const uint32_t hap = rg.hap_start + h;
-          const uint64_t base = region_out[g] + (uint64_t)h * rg.num_reads - rg.read_start;
           if (fp64) {
-            for (uint32_t rr : rd) *li++ = PairRef{hap, rr, (uint32_t)(base + rr)};
+            for (uint32_t rr : rd) *li++ = PairRef{hap, rr, out_of(h, rr)};
             continue;
           }
           size_t k = 0;
           for (; k + 1 < rd.size(); k += 2)
-            *si++ = SameItem{hap, rd[k], rd[k + 1], (uint32_t)(base + rd[k])};
-          if (k < rd.size()) *lf++ = PairRef{hap, rd[k], (uint32_t)(base + rd[k])};
+            *si++ = SameItem{hap, rd[k], rd[k + 1], out_of(h, rd[k])};
+          if (k < rd.size()) *lf++ = PairRef{hap, rd[k], out_of(h, rd[k])};
         }
       }
     }
@@ -480,10 +586,9 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   uint64_t cells = 0;
   for (uint32_t g = 0; g < G; ++g) {
     const rodv_region& rg = b.regions[g];
-    uint64_t hs = 0, rs = 0;
-    for (uint32_t h = 0; h < rg.num_haps; ++h) hs += b.hap_lengths[rg.hap_start + h];
+    uint64_t rs = 0;
     for (uint32_t r = 0; r < rg.num_reads; ++r) rs += b.read_lengths[rg.read_start + r];
-    cells += hs * rs;
+    cells += hsum[g] * rs;
   }
   plan.cells = cells;
   return RODV_OK;
@@ -706,16 +811,17 @@ rodv_status Engine::plain(rodv_device_batch* db, double* out, rodv_stats* st) {
   const PackedPlan& plan = db->plan;
   uint8_t* d = static_cast<uint8_t*>(db->arena.ptr);
   ArenaView a = arena_view(plan, d, tab_);
-  // control block: [0,16) SameItem, [16,28) rescue PairRef, words 8..11:
-  // fp32 counter, fp64 counter, rescue count, error flags
+  // control block: [0,24) ChainItem (one haplotype, one read) or SameItem
+  // (multi-pass), [32,44) rescue PairRef, words 12..15: fp32 counter, fp64
+  // counter, rescue count, error flags
   DeviceMem ctl;
   RODV_CUDA(ctl.ensure(64));
   uint8_t* w = static_cast<uint8_t*>(ctl.ptr);
-  uint32_t* wc = reinterpret_cast<uint32_t*>(w + 32);
+  uint32_t* wc = reinterpret_cast<uint32_t*>(w + 48);
   PinnedMem host;
   RODV_CUDA(host.ensure(64));
   uint8_t* hw = static_cast<uint8_t*>(host.ptr);
-  uint32_t* hc = reinterpret_cast<uint32_t*>(hw + 32);
+  uint32_t* hc = reinterpret_cast<uint32_t*>(hw + 48);
   uint32_t launches = 0;
   uint64_t rescued = 0;
   const auto t0 = std::chrono::steady_clock::now();
@@ -726,23 +832,28 @@ rodv_status Engine::plain(rodv_device_batch* db, double* out, rodv_stats* st) {
       for (uint32_t r = 0; r < rg.num_reads; ++r, ++p) {
         const uint32_t read = rg.read_start + r;
         const int c = plan.read_class[read];
-        const SameItem item{rg.hap_start + h, read, kNoPair, (uint32_t)p};
-        std::memcpy(hw, &item, sizeof(item));
+        if (class_multi(c)) {
+          const SameItem item{rg.hap_start + h, read, kNoPair, (uint32_t)p};
+          std::memcpy(hw, &item, sizeof(item));
+        } else {
+          const ChainItem item{rg.hap_start + h, 1, read, kNoPair, (uint32_t)p, 0};
+          std::memcpy(hw, &item, sizeof(item));
+        }
         const PairRef ref{rg.hap_start + h, read, (uint32_t)p};
-        std::memcpy(hw + 16, &ref, sizeof(ref));
+        std::memcpy(hw + 32, &ref, sizeof(ref));
         hc[0] = hc[1] = hc[2] = hc[3] = 0;
-        RODV_CUDA(cudaMemcpyAsync(w, hw, 48, cudaMemcpyHostToDevice, stream_));
+        RODV_CUDA(cudaMemcpyAsync(w, hw, 64, cudaMemcpyHostToDevice, stream_));
         for (int pass = 0; pass < 2; ++pass) {
           const bool f64 = pass == 1 || plan.fp64;
           const KernelInfo k =
               forward_kernel_info(f64 ? Precision::kF64 : Precision::kF32x2, class_rows(c),
                                   class_uniform(c), class_multi(c), true, variant_[c]);
           ClassLaunch cl{};
-          cl.work = f64 ? static_cast<const void*>(w + 16) : static_cast<const void*>(w);
+          cl.work = f64 ? static_cast<const void*>(w + 32) : static_cast<const void*>(w);
           cl.work_count = nullptr;
           cl.static_count = 1;
           cl.counter = f64 ? wc + 1 : wc;
-          cl.rescue_list = reinterpret_cast<PairRef*>(w + 16);
+          cl.rescue_list = reinterpret_cast<PairRef*>(w + 32);
           cl.rescue_count = wc + 2;
           cl.scratch = a.scratch;
           cl.scratch_cols = plan.scratch_cols;
@@ -779,10 +890,10 @@ rodv_status Engine::plain(rodv_device_batch* db, double* out, rodv_stats* st) {
 
 // ---------------------------------------------------------------------------
 // Autotuning: per work class, the occupancy variant (register budget) of the
-// same-haplotype FP32 kernel, chosen by timing every variant on a synthetic
-// batch of that class (reads of 32R-5 bases, or 700 for multi-pass, against
-// 400- or 1,200-base haplotypes; ~16 items per resident warp).  Results are
-// cached per device.
+// same-haplotype FP32 kernel (chain kernel for single-pass classes), chosen by
+// timing every variant on a synthetic batch of that class (reads of 32R-5
+// bases, or 700 for multi-pass, against four 400- or 1,200-base haplotypes
+// per region).  Results are cached per device.
 // ---------------------------------------------------------------------------
 std::string Engine::device_key() const {
   std::string k = device_name_;
@@ -832,13 +943,14 @@ rodv_status Engine::autotune(const char* cache_path, int force, int32_t* variant
     const bool multi = class_multi(c), uni = class_uniform(c);
     const uint32_t L = multi ? 700 : (uint32_t)std::max(1, 32 * R - 5);
     const uint32_t H = multi ? 1200 : 400;
-    // Enough items that every warp of the largest grid takes ~16 of them
-    // (4 for multi-pass), so the timing reflects per-item throughput and not
-    // the tail of the work queue.
+    // Enough items that every warp of the largest grid takes several (chain
+    // items of 4 haplotypes: ~8; multi-pass same-haplotype items: ~4), so the
+    // timing reflects per-item throughput and not the tail of the work queue.
     const uint64_t max_warps = (uint64_t)num_sms_ * kVariantMinBlocks[kTuneVariants - 1] * 4;
-    const uint64_t items = max_warps * (multi ? 4 : 16);
     const int regions = 16, haps = 4;
-    const int reads = (int)std::max<uint64_t>(2, 2 * items / (regions * haps) + 1);
+    const uint64_t items = max_warps * (multi ? 4 : 8);
+    const int reads = (int)std::max<uint64_t>(
+        2, (multi ? 2 * items / (regions * haps) : 2 * items / regions) + 1);
     std::vector<uint8_t> hb, rb, q, ins, del, gcp;
     std::vector<uint64_t> ho, ro;
     std::vector<uint32_t> hl, rl;
@@ -892,6 +1004,9 @@ rodv_status Engine::autotune(const char* cache_path, int force, int32_t* variant
         cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
         if (rep > 0) vbest = std::min(vbest, ms);
       }
+      if (opt_.verbose)
+        fprintf(stderr, "rodv: tune class %d R=%d%s%s variant %d (%d blocks/SM): %.3f ms\n", c,
+                R, uni ? " uniform" : "", multi ? " multi" : "", v, kVariantMinBlocks[v], vbest);
       if (vbest < best_ms) {
         best_ms = vbest;
         best_v = v;

@@ -65,9 +65,12 @@ struct PackedPlan {
   uint32_t max_hap_len = 0;
   uint32_t multi_max_hap = 0;
   bool fp64 = false;                       // every pair computed in FP64
-  uint32_t same_items[kNumClasses] = {};   // FP32 same-haplotype items
-  uint32_t diff_items[kNumClasses] = {};   // FP32 two-haplotype items (leftovers)
-  uint32_t pairs[kNumClasses] = {};        // pairs per class
+  // FP32 same-haplotype items: ChainItem for single-pass classes, SameItem
+  // for the multi-pass ones
+  uint32_t same_items[kNumClasses] = {};
+  uint32_t diff_items[kNumClasses] = {};   // FP32 two-haplotype items (multi-pass leftovers)
+  uint32_t chain_haps[kNumClasses] = {};   // haplotypes per chain item (single-pass classes)
+  uint32_t pairs[kNumClasses] = {};        // pairs per class (FP64 list capacity)
   size_t off_hap_codes = 0, off_read_rows = 0, off_haps = 0, off_reads = 0;
   size_t off_same[kNumClasses] = {};
   size_t off_diff[kNumClasses] = {};

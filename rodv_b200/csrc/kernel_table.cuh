@@ -17,10 +17,11 @@ KernelInfo make_info(int variant) {
   k.fn = reinterpret_cast<const void*>(&forward_kernel<P, R, U, MU, SAME, MINB>);
   k.threads = F::kWarpsPerBlock * kWarp;
   k.warps_per_block = F::kWarpsPerBlock;
-  k.smem_bytes = F::kWarpsPerBlock * TableShape<P, R, SAME>::kBytesPerWarp;
+  k.smem_bytes = F::kWarpsPerBlock * F::kSmemPerWarp;
   k.rows_per_lane = R;
   k.multi = MU;
   k.same_hap = SAME || P::kSlots == 1;
+  k.chain = F::kChain;
   k.min_blocks = MINB;
   k.variant = variant;
   return k;
@@ -30,12 +31,16 @@ KernelInfo make_info(int variant) {
 // (kVariantMinBlocks); every other kernel has one variant.
 template <class P, int R, bool U, bool MU, bool SAME>
 KernelInfo variant_info(int variant) {
-  if (!(std::is_same<P, F32x2>::value && SAME)) return make_info<P, R, U, MU, SAME, 1>(0);
-  switch (variant) {
-    case 0: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[0]>(0);
-    case 1: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[1]>(1);
-    case 2: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[2]>(2);
-    default: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[3]>(3);
+  if constexpr (!(std::is_same<P, F32x2>::value && SAME)) {
+    (void)variant;
+    return make_info<P, R, U, MU, SAME, 1>(0);
+  } else {
+    switch (variant) {
+      case 0: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[0]>(0);
+      case 1: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[1]>(1);
+      case 2: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[2]>(2);
+      default: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[3]>(3);
+    }
   }
 }
 
@@ -47,8 +52,15 @@ KernelInfo info_for(Precision prec, bool uniform, bool same, int variant) {
   if (same)
     return uniform ? variant_info<F32x2, R, true, MU, true>(variant)
                    : variant_info<F32x2, R, false, MU, true>(variant);
-  return uniform ? variant_info<F32x2, R, true, MU, false>(0)
-                 : variant_info<F32x2, R, false, MU, false>(0);
+  // Two-haplotype items exist for multi-pass reads only (single-pass reads
+  // of a region all go into chain items).
+  if constexpr (MU) {
+    return uniform ? variant_info<F32x2, R, true, MU, false>(0)
+                   : variant_info<F32x2, R, false, MU, false>(0);
+  } else {
+    (void)uniform;
+    return KernelInfo{};
+  }
 }
 
 }  // namespace rodv

@@ -14,6 +14,7 @@ struct KernelInfo {
   int rows_per_lane = 0;      // R
   bool multi = false;         // sweeps reads longer than 32*R rows in passes
   bool same_hap = false;      // both pairs of an item share the haplotype
+  bool chain = false;         // takes ChainItem work (single-pass same-haplotype FP32)
   int min_blocks = 1;         // launch-bounds occupancy target (caps registers)
   int variant = 0;
 };
@@ -23,9 +24,11 @@ constexpr int kTuneVariants = 4;
 constexpr int kVariantMinBlocks[kTuneVariants] = {4, 5, 6, 8};
 
 // Forward kernel for one work class.  rows_per_lane in 1..8; multi kernels
-// always use 8 rows per lane.  same: items whose two pairs share the
-// haplotype (FP32 only; FP64 items hold one pair).  variant < kTuneVariants
-// selects the occupancy target of same-haplotype FP32 kernels.
+// always use 8 rows per lane.  same: FP32 items whose reads share the
+// haplotypes -- ChainItem for single-pass classes, SameItem for multi-pass
+// ones; !same: DiffItem (multi-pass only; fn is null for a single-pass class).
+// FP64 kernels take PairRef lists.  variant < kTuneVariants selects the
+// occupancy target of same-haplotype FP32 kernels.
 KernelInfo forward_kernel_info(Precision prec, int rows_per_lane, bool uniform, bool multi,
                                bool same = true, int variant = 0);
 inline int forward_kernel_variants(Precision prec, bool same) {

@@ -3,19 +3,24 @@
 // A batch is packed once on the host into these flat arrays (one H2D copy
 // each) and stays resident in HBM while the kernels run:
 //
-//   hap_codes  u8   every haplotype as base codes A0 C1 G2 T3 N4, preceded
-//                   and followed by kHapPad code-0 bytes; the buffer tail
-//                   holds kHapPad + max_hap_len more, so a warp whose shorter
-//                   slot runs past its haplotype end still reads in bounds.
+//   hap_codes  u8   the haplotypes in batch order as base codes A0 C1 G2 T3
+//                   N4, one separator code (kSep) between consecutive
+//                   haplotypes, kHapPad code-0 bytes before the first; the
+//                   tail holds kHapPad + max_hap_len + kHapPad more, so a warp
+//                   whose shorter slot runs past its haplotype end still
+//                   reads in bounds.  Any run of consecutive haplotypes is
+//                   therefore one column sequence [h0][sep][h1][sep]...
 //   read_rows  u32  one word per read base:
 //                     bits 0-2 base code, 3-9 q, 10-16 ins, 17-23 del,
 //                     24-30 gcp (quals masked with &127 as the reference
 //                     does, pairhmm_inter.cpp:85-88); each read starts on a
 //                     16-byte boundary.
 //   haps       HapDesc[], reads ReadDesc[]
-//   items      the FP32 kernels' work, two pairs per warp (the two float
-//              halves of every f32x2 instruction): SameItem (two reads against
-//              one haplotype) or a DiffItem (two PairRef) for the leftovers
+//   items      the FP32 kernels' work, two reads per warp (the two float
+//              halves of every f32x2 instruction): ChainItem (two reads
+//              against all haplotypes of their region, single-pass reads),
+//              SameItem (two reads against one haplotype, multi-pass reads) or
+//              DiffItem (two PairRef, the multi-pass leftovers)
 //   lists      PairRef[] per work class: the FP64 kernels' work (pairs the
 //              FP32 kernels rescued, or every pair when FP64 is forced)
 //   out        f64[num_pairs]  final log10 likelihood, in the reference's
@@ -32,14 +37,18 @@
 namespace rodv {
 
 constexpr int kWarp = 32;
-constexpr int kHapPad = 32;          // code bytes before/after each haplotype
+constexpr int kHapPad = 32;          // code bytes before the first haplotype
+constexpr int kChainHaps = 32;       // haplotypes per chain item (one per lane)
 constexpr int kMaxRowsPerLane = 8;   // R: read rows held in registers per lane
 constexpr int kPassRows = kWarp * kMaxRowsPerLane;  // rows per multi-pass sweep
 constexpr uint32_t kNoPair = 0xffffffffu;
 
 // Base codes.  'N' on either side matches every base (common.h:42-56,
 // pairhmm_impl.cpp:26-42).
-enum BaseCode : uint8_t { kA = 0, kC = 1, kG = 2, kT = 3, kN = 4 };
+// kSep is the column between two haplotypes of a chain: its emission is 0 for
+// every row.
+enum BaseCode : uint8_t { kA = 0, kC = 1, kG = 2, kT = 3, kN = 4, kSep = 5 };
+constexpr int kNumCodes = 6;
 
 struct HapDesc {
   uint64_t code_off;  // index in hap_codes of the first base
@@ -69,6 +78,19 @@ struct SameItem {
   uint32_t read_x;
   uint32_t read_y;
   uint32_t out_x;
+};
+
+// Two reads of one region against every haplotype of the region, swept in
+// one pass over the concatenated haplotype columns.  The result of
+// (haplotype hap_start + i, read_x) goes to out_x + i * stride; read_y's to
+// that index + (read_y - read_x).  read_y may be kNoPair.
+struct ChainItem {
+  uint32_t hap_start;
+  uint32_t num_haps;
+  uint32_t read_x;
+  uint32_t read_y;
+  uint32_t out_x;
+  uint32_t stride;    // the region's read count
 };
 
 // Two arbitrary pairs; x has the longer (or equal) haplotype; y.read may be
@@ -126,6 +148,7 @@ struct ClassLaunch {
 enum ErrorFlag : uint32_t {
   kErrBadLength = 1u,   // a pair with zero or over-limit length reached a kernel
   kErrPassLimit = 2u,   // a read longer than the pass limit reached a kernel
+  kErrChain = 4u,       // a chain item with no haplotypes
 };
 
 }  // namespace rodv

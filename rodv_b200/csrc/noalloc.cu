@@ -393,6 +393,9 @@ extern "C" rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32
 
   using F32 = Forward<F32x2, kMaxRowsPerLane, false, true, false, 1>;
   using D64 = Forward<F64, kMaxRowsPerLane, false, true, false, 1>;
+  // launched without the dynamic shared-memory opt-in
+  static_assert(F32::kWarpsPerBlock * F32::kSmemPerWarp <= 48 * 1024, "F32 table too large");
+  static_assert(D64::kWarpsPerBlock * D64::kSmemPerWarp <= 48 * 1024, "F64 table too large");
   ClassLaunch c32{};
   c32.work = s + kOffItems;
   c32.work_count = cnt + kCItems;
@@ -404,7 +407,7 @@ extern "C" rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32
   c32.error_flags = cnt + kCErr;
   forward_kernel<F32x2, kMaxRowsPerLane, false, true, false, 1>
       <<<kNaBlocks, F32::kWarpsPerBlock * kWarp,
-         F32::kWarpsPerBlock * TableShape<F32x2, kMaxRowsPerLane, false>::kBytesPerWarp, st>>>(
+         F32::kWarpsPerBlock * F32::kSmemPerWarp, st>>>(
           v, c32);
   ClassLaunch c64 = c32;
   c64.work = s + kOffList;
@@ -414,7 +417,7 @@ extern "C" rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32
   c64.rescue_count = nullptr;
   forward_kernel<F64, kMaxRowsPerLane, false, true, false, 1>
       <<<kNaBlocks, D64::kWarpsPerBlock * kWarp,
-         D64::kWarpsPerBlock * TableShape<F64, kMaxRowsPerLane, false>::kBytesPerWarp, st>>>(
+         D64::kWarpsPerBlock * D64::kSmemPerWarp, st>>>(
           v, c64);
   if (cudaGetLastError() != cudaSuccess) return RODV_ERR_CUDA;
 

@@ -146,13 +146,14 @@ __device__ __forceinline__ RowPriors<S> row_priors(uint32_t w, const PriorTables
   return p;
 }
 
-// Shared-memory shape of one warp's emission tables for R rows per lane.
+// Shared-memory shape of one warp's emission tables for R rows per lane
+// (kNumCodes codes; the separator code's entries are all 0).
 //   SAME layout (F64 always, F32x2 same-haplotype items): element (code, k)
 //     is one V; a 16-byte vector holds rows k, k+1 of the lane:
 //     vec index ((code * kNv + k/2) * 32 + lane).
 //   DIFF layout (F32x2 two-haplotype items): per slot, element (slot, code, k)
 //     is one float; a 16-byte vector holds rows k..k+3 of the lane:
-//     vec index (((slot * 5 + code) * kNv + k/4) * 32 + lane).
+//     vec index (((slot * kNumCodes + code) * kNv + k/4) * 32 + lane).
 template <class P, int R, bool SAME>
 struct TableShape {
   static constexpr bool kSameLayout = SAME || P::kSlots == 1;
@@ -160,7 +161,7 @@ struct TableShape {
   static constexpr int kRq = (R + kRowsPerVec - 1) / kRowsPerVec * kRowsPerVec;
   static constexpr int kNv = kRq / kRowsPerVec;  // 16-byte loads per code (per slot)
   static constexpr int kTables = kSameLayout ? 1 : 2;
-  static constexpr int kBytesPerWarp = kTables * 5 * kNv * kWarp * 16;
+  static constexpr int kBytesPerWarp = kTables * kNumCodes * kNv * kWarp * 16;
 };
 
 // Per-slot state of the pair being computed.
@@ -168,8 +169,14 @@ struct SlotInfo {
   const uint8_t* hap;   // first base code of the haplotype
   uint32_t H, L;
   uint64_t row_off;
-  PairRef ref;
-  bool valid;
+};
+
+// Per-warp shared memory of a chain sweep beyond the emission table: the
+// column of the separator after each haplotype, and lane 31's two running
+// sums (M, I of the last read row; x and y halves) at the end of each one.
+struct ChainMeta {
+  float4 acc[kChainHaps];
+  uint32_t sep[kChainHaps];
 };
 
 template <class P, int R, bool UNIFORM, bool MULTI, bool SAME, int MINB>
@@ -178,11 +185,22 @@ struct Forward {
   using S = typename P::S;
   using Shape = TableShape<P, R, SAME>;
   static constexpr bool kSameHap = Shape::kSameLayout;
+  // Single-pass same-haplotype FP32 kernels take chain items.
+  static constexpr bool kChain = SAME && !MULTI && P::kSlots == 2;
   static constexpr int kWarpsPerBlock = 4;
+  static constexpr int kSmemPerWarp = Shape::kBytesPerWarp + (kChain ? (int)sizeof(ChainMeta) : 0);
 
   // Boundary row written by lane 31 of one pass and read by lane 0 of the next.
   struct BoundaryCell {
     V m, i, d;
+  };
+
+  // Transition priors of this lane's R rows (per row, or the read's uniform
+  // values), both slots packed.
+  struct Priors {
+    V mm[UNIFORM ? 1 : R], gapm[UNIFORM ? 1 : R], md[UNIFORM ? 1 : R];
+    V mi[R], ii[R];
+    V mmU, mdU, ddU;
   };
 
   // Writes emission e of (slot, code, row k) into this lane's table.
@@ -193,14 +211,140 @@ struct Forward {
       // 16-byte vector = 2 rows of V; V = S[kSlots]
       tab[vec * (16 / (int)sizeof(S)) + (k % 2) * P::kSlots + slot] = e;
     } else {
-      const int vec = ((slot * 5 + code) * Shape::kNv + k / 4) * kWarp + lane;
+      const int vec = ((slot * kNumCodes + code) * Shape::kNv + k / 4) * kWarp + lane;
       tab[vec * 4 + (k % 4)] = e;
     }
   }
 
-  __device__ static void run_item(const BatchView& b, const ClassLaunch& c, uint32_t item,
-                                  int lane, int gwarp, uint4* table) {
-    PairRef refs[2];
+  // Emission tables and priors for read rows pass*32R + lane*R + [0, R) of
+  // the two slots (reads of L[s] rows starting at row word row_off[s]).
+  // Rows past a read's end are pass-through rows: emission 0, mi = ii = 1,
+  // md = 0 (in the uniform form mi*gapm = gapm, since M~ = M/gapm).
+  __device__ __forceinline__ static void load_rows(const BatchView& b, const uint32_t (&L)[2],
+                                                   const uint64_t (&row_off)[2], uint32_t pass,
+                                                   int lane, uint4* table, Priors& p) {
+    RowPriors<S> u[2];
+    if (UNIFORM) {  // uniform-gap priors come from the read's first row
+      u[0] = row_priors<S>(b.read_rows[row_off[0]], b.tab);
+      u[1] = row_priors<S>(b.read_rows[row_off[1]], b.tab);
+      p.mmU = P::make(u[0].mm, u[1].mm);
+      p.mdU = P::make(u[0].md * u[0].gapm, u[1].md * u[1].gapm);
+      p.ddU = P::make(u[0].ii, u[1].ii);
+    }
+    S* tab = reinterpret_cast<S*>(table);
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const uint32_t row = pass * (kWarp * R) + lane * R + k;  // 0-based read row
+      S mmv[2], gv[2], miv[2], iiv[2], mdv[2];
+#pragma unroll
+      for (int s = 0; s < P::kSlots; ++s) {
+        const bool real = row < L[s];
+        const uint32_t w = real ? b.read_rows[row_off[s] + row] : 0u;
+        const RowPriors<S> rp = row_priors<S>(w, b.tab);
+        const uint32_t rc = rw_code(w);
+#pragma unroll
+        for (int code = 0; code < kN + 1; ++code) {
+          const bool hit = (rc == (uint32_t)code) || rc == kN || code == kN;
+          put_emission(tab, s, code, k, lane, real ? (hit ? rp.match : rp.mismatch) : S(0));
+        }
+        put_emission(tab, s, kSep, k, lane, S(0));
+        if (UNIFORM) {
+          miv[s] = real ? u[s].mi * u[s].gapm : u[s].gapm;
+          iiv[s] = real ? u[s].ii : S(1);
+        } else {
+          mmv[s] = real ? rp.mm : S(0);
+          gv[s] = real ? rp.gapm : S(0);
+          miv[s] = real ? rp.mi : S(1);
+          iiv[s] = real ? rp.ii : S(1);
+          mdv[s] = real ? rp.md : S(0);
+        }
+      }
+      if (P::kSlots == 1) {
+        miv[1] = miv[0]; iiv[1] = iiv[0];
+        mmv[1] = mmv[0]; gv[1] = gv[0]; mdv[1] = mdv[0];
+      }
+      p.mi[k] = P::make(miv[0], miv[1]);
+      p.ii[k] = P::make(iiv[0], iiv[1]);
+      if (!UNIFORM) {
+        p.mm[UNIFORM ? 0 : k] = P::make(mmv[0], mmv[1]);
+        p.gapm[UNIFORM ? 0 : k] = P::make(gv[0], gv[1]);
+        p.md[UNIFORM ? 0 : k] = P::make(mdv[0], mdv[1]);
+      }
+    }
+  }
+
+  // Emission values of this lane's rows for haplotype codes cx (slot x) and
+  // cy (slot y; used by the DIFF layout only).
+  __device__ __forceinline__ static void load_emission(const uint4* table, int lane, uint32_t cx,
+                                                       uint32_t cy, V (&e)[R]) {
+    if (kSameHap) {
+      const uint4* px = table + lane + cx * (Shape::kNv * kWarp);
+#pragma unroll
+      for (int v = 0; v < Shape::kNv; ++v) {
+        const uint4 raw = px[v * kWarp];
+        const V* f = reinterpret_cast<const V*>(&raw);
+        if (2 * v < R) e[2 * v] = f[0];
+        if (2 * v + 1 < R) e[2 * v + 1] = f[1];
+      }
+    } else {
+      S ex[Shape::kRq], ey[Shape::kRq];
+      const uint4* px = table + lane + cx * (Shape::kNv * kWarp);
+      const uint4* py = table + kNumCodes * Shape::kNv * kWarp + lane + cy * (Shape::kNv * kWarp);
+#pragma unroll
+      for (int v = 0; v < Shape::kNv; ++v) {
+        const uint4 rx = px[v * kWarp], ry = py[v * kWarp];
+        const S* fx = reinterpret_cast<const S*>(&rx);
+        const S* fy = reinterpret_cast<const S*>(&ry);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          ex[v * 4 + q] = fx[q];
+          ey[v * 4 + q] = fy[q];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < R; ++k) e[k] = P::make(ex[k], ey[k]);
+    }
+  }
+
+  // One column of this lane's R rows.  (M, I, D)[k] hold the previous
+  // column on entry (the left neighbours) and this column on exit; dg is the
+  // row above the lane's first row at the previous column, up the same row
+  // at this column.
+  __device__ __forceinline__ static void cells(const V (&e)[R], V up_m, V up_i, V up_d, V& dg_m,
+                                               V& dg_i, V& dg_d, V (&M)[R], V (&I)[R], V (&D)[R],
+                                               const Priors& p) {
+    V dm = dg_m, di = dg_i, dd = dg_d, um = up_m, ui = up_i;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const V oM = M[k], oI = I[k], oD = D[k];
+      V t = P::add(di, dd);
+      if (UNIFORM) {
+        t = P::fma(p.mmU, dm, t);
+      } else {
+        t = P::mul(p.gapm[k], t);
+        t = P::fma(p.mm[k], dm, t);
+      }
+      if (kSameHap) {
+        M[k] = P::mul(t, e[k]);
+      } else {
+        M[k] = P::make(P::sx(t) * P::sx(e[k]), P::sy(t) * P::sy(e[k]));
+      }
+      I[k] = P::fma(p.ii[k], ui, P::mul(p.mi[k], um));
+      if (UNIFORM) {
+        D[k] = P::fma(p.ddU, oD, P::mul(p.mdU, oM));
+      } else {
+        D[k] = P::fma(p.ii[k], oD, P::mul(p.md[k], oM));
+      }
+      dm = oM; di = oI; dd = oD;
+      um = M[k]; ui = I[k];
+    }
+    dg_m = up_m; dg_i = up_i; dg_d = up_d;
+  }
+
+  // The two pairs of work item `item` (the second one's read is kNoPair when
+  // the item holds one pair).
+  __device__ __forceinline__ static void load_refs(const ClassLaunch& c, uint32_t item,
+                                                   PairRef refs[2]) {
     if (P::kSlots == 1) {
       refs[0] = static_cast<const PairRef*>(c.work)[item];
       refs[1] = refs[0];
@@ -214,6 +358,20 @@ struct Forward {
       refs[0] = it.x;
       refs[1] = it.y;
     }
+  }
+
+  // gapm of a uniform-gap read (every row has the same gcp quality).
+  __device__ __forceinline__ static S uniform_gapm(const BatchView& b, uint32_t read) {
+    const uint32_t w = b.read_rows[b.reads[read].row_off];
+    return S(1) - __ldg(Tables<S>::ph2pr(b.tab) + rw_gcp(w));
+  }
+
+  // One pair per slot (SameItem, DiffItem or, for F64, PairRef), swept in one
+  // or (MULTI) several passes of 32R rows.
+  __device__ static void run_item(const BatchView& b, const ClassLaunch& c, uint32_t item,
+                                  int lane, int gwarp, uint4* table) {
+    PairRef refs[2];
+    load_refs(c, item, refs);
     SlotInfo sl[2];
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
@@ -225,8 +383,6 @@ struct Forward {
       sl[s].H = hd.len;
       sl[s].L = rd.len;
       sl[s].row_off = rd.row_off;
-      sl[s].ref = r;
-      sl[s].valid = valid;
     }
     const uint32_t Lmax = sl[0].L > sl[1].L ? sl[0].L : sl[1].L;
     const uint32_t passes = MULTI ? (Lmax + kWarp * R - 1) / (kWarp * R) : 1;
@@ -239,14 +395,8 @@ struct Forward {
     const int nsteps = (int)sl[0].H + kWarp - 1;    // slot x has the longer haplotype
     const int nfreeze = (int)sl[1].H + kWarp - 1;   // slot y's last accumulated step + 1
     const V init = P::make(P::init_const() / (S)sl[0].H, P::init_const() / (S)sl[1].H);
-
-    // Uniform-gap priors come from the read's first row.
-    const RowPriors<S> u0 = row_priors<S>(b.read_rows[sl[0].row_off], b.tab);
-    const RowPriors<S> u1 = row_priors<S>(b.read_rows[sl[1].row_off], b.tab);
-    const V gapmU = P::make(u0.gapm, u1.gapm);
-    const V mmU = P::make(u0.mm, u1.mm);
-    const V mdU = P::make(u0.md * u0.gapm, u1.md * u1.gapm);
-    const V ddU = P::make(u0.ii, u1.ii);
+    const uint32_t L[2] = {sl[0].L, sl[1].L};
+    const uint64_t row_off[2] = {sl[0].row_off, sl[1].row_off};
 
     BoundaryCell* buf = nullptr;
     if (MULTI) buf = reinterpret_cast<BoundaryCell*>(c.scratch) + (size_t)gwarp * c.scratch_cols;
@@ -256,59 +406,14 @@ struct Forward {
 
     for (uint32_t pass = 0; pass < passes; ++pass) {
       const bool last = (pass + 1 == passes);
-      // ---- per-row priors and emission tables for this lane's R rows ----
-      V pmm[UNIFORM ? 1 : R], pgapm[UNIFORM ? 1 : R], pmd[UNIFORM ? 1 : R];
-      V pmi[R], pii[R];
-      S* tab = reinterpret_cast<S*>(table);
-#pragma unroll
-      for (int k = 0; k < R; ++k) {
-        const uint32_t row = pass * (kWarp * R) + lane * R + k;  // 0-based read row
-        S mmv[2], gv[2], miv[2], iiv[2], mdv[2];
-#pragma unroll
-        for (int s = 0; s < P::kSlots; ++s) {
-          const bool real = row < sl[s].L;
-          const uint32_t w = real ? b.read_rows[sl[s].row_off + row] : 0u;
-          const RowPriors<S> rp = row_priors<S>(w, b.tab);
-          const uint32_t rc = rw_code(w);
-#pragma unroll
-          for (int code = 0; code < 5; ++code) {
-            const bool hit = (rc == (uint32_t)code) || rc == kN || code == kN;
-            put_emission(tab, s, code, k, lane, real ? (hit ? rp.match : rp.mismatch) : S(0));
-          }
-          if (UNIFORM) {
-            const RowPriors<S>& up = (s == 0) ? u0 : u1;
-            miv[s] = real ? up.mi * up.gapm : up.gapm;
-            iiv[s] = real ? up.ii : S(1);
-          } else {
-            mmv[s] = real ? rp.mm : S(0);
-            gv[s] = real ? rp.gapm : S(0);
-            miv[s] = real ? rp.mi : S(1);
-            iiv[s] = real ? rp.ii : S(1);
-            mdv[s] = real ? rp.md : S(0);
-          }
-        }
-        if (P::kSlots == 1) {
-          miv[1] = miv[0]; iiv[1] = iiv[0];
-          mmv[1] = mmv[0]; gv[1] = gv[0]; mdv[1] = mdv[0];
-        }
-        pmi[k] = P::make(miv[0], miv[1]);
-        pii[k] = P::make(iiv[0], iiv[1]);
-        if (!UNIFORM) {
-          pmm[UNIFORM ? 0 : k] = P::make(mmv[0], mmv[1]);
-          pgapm[UNIFORM ? 0 : k] = P::make(gv[0], gv[1]);
-          pmd[UNIFORM ? 0 : k] = P::make(mdv[0], mdv[1]);
-        }
-      }
+      Priors pr;
+      load_rows(b, L, row_off, pass, lane, table, pr);
 
-      // ---- sweep ----
       V M[R], I[R], D[R];
 #pragma unroll
       for (int k = 0; k < R; ++k) M[k] = I[k] = D[k] = P::zero();
       V dg_m = P::zero(), dg_i = P::zero(), dg_d = P::zero();
       if (lane == 0 && pass == 0) dg_d = init;
-      const V top_const_d = init;
-      const uint4* tab_x = table + lane;
-      const uint4* tab_y = table + 5 * Shape::kNv * kWarp + lane;
       const uint8_t* hx = sl[0].hap - lane;
       const uint8_t* hy = sl[1].hap - lane;
 
@@ -322,67 +427,12 @@ struct Forward {
             const BoundaryCell cell = buf[s + 1];
             up_m = cell.m; up_i = cell.i; up_d = cell.d;
           } else {
-            up_m = P::zero(); up_i = P::zero(); up_d = top_const_d;
+            up_m = P::zero(); up_i = P::zero(); up_d = init;
           }
         }
-        // emission values of this lane's rows for its current column
         V e[R];
-        if (kSameHap) {
-          const uint32_t cx = hx[s];
-          const uint4* px = tab_x + cx * (Shape::kNv * kWarp);
-#pragma unroll
-          for (int v = 0; v < Shape::kNv; ++v) {
-            const uint4 raw = px[v * kWarp];
-            const V* f = reinterpret_cast<const V*>(&raw);
-            if (2 * v < R) e[2 * v] = f[0];
-            if (2 * v + 1 < R) e[2 * v + 1] = f[1];
-          }
-        } else {
-          S ex[Shape::kRq], ey[Shape::kRq];
-          const uint32_t cx = hx[s];
-          const uint4* px = tab_x + cx * (Shape::kNv * kWarp);
-          const uint32_t cy = hy[s];
-          const uint4* py = tab_y + cy * (Shape::kNv * kWarp);
-#pragma unroll
-          for (int v = 0; v < Shape::kNv; ++v) {
-            const uint4 rx = px[v * kWarp], ry = py[v * kWarp];
-            const S* fx = reinterpret_cast<const S*>(&rx);
-            const S* fy = reinterpret_cast<const S*>(&ry);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              ex[v * 4 + q] = fx[q];
-              ey[v * 4 + q] = fy[q];
-            }
-          }
-#pragma unroll
-          for (int k = 0; k < R; ++k) e[k] = P::make(ex[k], ey[k]);
-        }
-        V dm = dg_m, di = dg_i, dd = dg_d, um = up_m, ui = up_i;
-#pragma unroll
-        for (int k = 0; k < R; ++k) {
-          const V oM = M[k], oI = I[k], oD = D[k];
-          V t = P::add(di, dd);
-          if (UNIFORM) {
-            t = P::fma(mmU, dm, t);
-          } else {
-            t = P::mul(pgapm[k], t);
-            t = P::fma(pmm[k], dm, t);
-          }
-          if (kSameHap) {
-            M[k] = P::mul(t, e[k]);
-          } else {
-            M[k] = P::make(P::sx(t) * P::sx(e[k]), P::sy(t) * P::sy(e[k]));
-          }
-          I[k] = P::fma(pii[k], ui, P::mul(pmi[k], um));
-          if (UNIFORM) {
-            D[k] = P::fma(ddU, oD, P::mul(mdU, oM));
-          } else {
-            D[k] = P::fma(pii[k], oD, P::mul(pmd[k], oM));
-          }
-          dm = oM; di = oI; dd = oD;
-          um = M[k]; ui = I[k];
-        }
-        dg_m = up_m; dg_i = up_i; dg_d = up_d;
+        load_emission(table, lane, hx[s], kSameHap ? 0u : (uint32_t)hy[s], e);
+        cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr);
         if (MULTI && !last && lane == kWarp - 1) {
           const int col = s - (kWarp - 1) + 1;
           if (col >= 1 && col <= (int)sl[0].H) {
@@ -408,33 +458,159 @@ struct Forward {
       frozen_m = P::sy(acc_m);
       frozen_i = P::sy(acc_i);
     }
+    // Values needed only now are re-read rather than kept live in registers
+    // through the sweep.
+    PairRef fr[2];
+    load_refs(c, item, fr);
+    const bool valid_y = P::kSlots == 2 && fr[1].read != kNoPair;
     S res[2];
-    res[0] = UNIFORM ? P::sx(gapmU) * P::sx(acc_m) + P::sx(acc_i) : P::sx(acc_m) + P::sx(acc_i);
-    if (P::kSlots == 2)
-      res[1] = UNIFORM ? P::sy(gapmU) * frozen_m + frozen_i : frozen_m + frozen_i;
-#pragma unroll
-    for (int s = 0; s < P::kSlots; ++s) {
-      if (!sl[s].valid) continue;
-      finish(b, c, sl[s], res[s]);
+    if (UNIFORM) {
+      res[0] = uniform_gapm(b, fr[0].read) * P::sx(acc_m) + P::sx(acc_i);
+      if (valid_y) res[1] = uniform_gapm(b, fr[1].read) * frozen_m + frozen_i;
+    } else {
+      res[0] = P::sx(acc_m) + P::sx(acc_i);
+      res[1] = frozen_m + frozen_i;
     }
+    finish(b, c, fr[0], (double)res[0]);
+    if (valid_y) finish(b, c, fr[1], (double)res[1]);
   }
 
-  // FP32 result: accepted at >= 1e-28 with an FP64 log10, else queued for FP64.
-  __device__ static void finish(const BatchView& b, const ClassLaunch& c, const SlotInfo& sl,
-                                S raw) {
+  // A chain item: reads x and y against haplotypes hap_start .. +num_haps-1,
+  // swept as one column sequence h0 sep h1 sep ... (the packed layout of
+  // consecutive haplotypes).  Each lane crosses a separator one step after
+  // its left neighbour; the separator column is the next haplotype's
+  // column 0:
+  //   M = 0 there (its emission is 0 for every row),
+  //   I = 0 there (the column above it is 0 down from row 0),
+  //   D is set to 0 by the lane after it computes the separator column.
+  // So every haplotype sees the reference's column-0 boundary, and the
+  // wavefront fills and drains once per chain instead of once per pair.
+  // Row 0 uses one scaling constant for the whole chain, 2^120/Hmax; the DP
+  // is linear in it, so haplotype i's result is rescaled by
+  // (2^120/H_i)/(2^120/Hmax) in FP64 before the acceptance test and log10.
+  __device__ static void run_chain(const BatchView& b, const ClassLaunch& c, uint32_t item,
+                                   int lane, uint4* table) {
+    ChainMeta* meta = reinterpret_cast<ChainMeta*>(table + Shape::kBytesPerWarp / 16);
+    const ChainItem it = static_cast<const ChainItem*>(c.work)[item];
+    const bool has_y = it.read_y != kNoPair;
+    const uint32_t n = it.num_haps;
+    const ReadDesc rx = b.reads[it.read_x];
+    const ReadDesc ry = b.reads[has_y ? it.read_y : it.read_x];
+    // lane i holds haplotype i's length and code offset
+    uint32_t hl = 0;
+    uint64_t co = 0;
+    if ((uint32_t)lane < n && n <= (uint32_t)kChainHaps) {
+      const HapDesc hd = b.haps[it.hap_start + lane];
+      hl = hd.len;
+      co = hd.code_off;
+    }
+    const uint64_t co_next = __shfl_down_sync(kFullMask, co, 1);
+    const bool bad_hap = (uint32_t)lane < n && (hl == 0 || ((uint32_t)lane + 1 < n &&
+                                                            co_next != co + hl + 1));
+    const uint32_t Lmax = rx.len > ry.len ? rx.len : ry.len;
+    if (__any_sync(kFullMask, bad_hap) || n == 0 || n > (uint32_t)kChainHaps || rx.len == 0 ||
+        ry.len == 0 || Lmax > (uint32_t)(kWarp * R)) {
+      if (lane == 0) atomicOr(c.error_flags, kErrChain);
+      return;
+    }
+    // end column (exclusive) + 1 of haplotype `lane` in the chain's columns
+    uint32_t endc = (uint32_t)lane < n ? hl + 1 : 0;
+    uint32_t hmax = hl;
+#pragma unroll
+    for (int d = 1; d < kWarp; d *= 2) {
+      const uint32_t v = __shfl_up_sync(kFullMask, endc, d);
+      if (lane >= d) endc += v;
+      hmax = max(hmax, __shfl_xor_sync(kFullMask, hmax, d));
+    }
+    constexpr uint32_t kNever = 0x40000000u;  // beyond every chain's last step
+    meta->sep[lane] = ((uint32_t)lane + 1 < n) ? endc - 1 : kNever;
+    const uint32_t ncols = __shfl_sync(kFullMask, endc, (int)n - 1) - 1;  // sum H + n - 1
+    const uint64_t co0 = __shfl_sync(kFullMask, co, 0);
+    const S init_s = P::init_const() / (S)hmax;
+    const V init = P::make(init_s, init_s);
+    const uint32_t L[2] = {rx.len, ry.len};
+    const uint64_t row_off[2] = {rx.row_off, ry.row_off};
+    Priors pr;
+    load_rows(b, L, row_off, 0, lane, table, pr);
+    __syncwarp();
+
+    V M[R], I[R], D[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) M[k] = I[k] = D[k] = P::zero();
+    V dg_m = P::zero(), dg_i = P::zero(), dg_d = P::zero();
+    if (lane == 0) dg_d = init;
+    const uint8_t* hx = b.hap_codes + co0 - lane;
+    uint32_t hi = 0;                          // this lane's haplotype in the chain
+    int nxt = (int)meta->sep[0] + lane;       // step at which this lane is at the next separator
+    V acc_m = P::zero(), acc_i = P::zero();
+    const int nsteps = (int)ncols + kWarp - 1;
+
+#pragma unroll 2
+    for (int s = 0; s < nsteps; ++s) {
+      V up_m = P::shfl_up(M[R - 1]);
+      V up_i = P::shfl_up(I[R - 1]);
+      V up_d = P::shfl_up(D[R - 1]);
+      if (lane == 0) {
+        up_m = P::zero(); up_i = P::zero(); up_d = init;
+      }
+      V e[R];
+      load_emission(table, lane, hx[s], 0u, e);
+      cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr);
+      acc_m = P::add(acc_m, M[R - 1]);
+      acc_i = P::add(acc_i, I[R - 1]);
+      if (s == nxt) {  // this lane just computed a separator column
+#pragma unroll
+        for (int k = 0; k < R; ++k) D[k] = P::zero();
+        if (lane == kWarp - 1) {
+          meta->acc[hi] = make_float4(P::sx(acc_m), P::sy(acc_m), P::sx(acc_i), P::sy(acc_i));
+          acc_m = P::zero();
+          acc_i = P::zero();
+        }
+        ++hi;
+        nxt = (int)meta->sep[hi] + lane;
+      }
+    }
+    if (lane == kWarp - 1)
+      meta->acc[n - 1] = make_float4(P::sx(acc_m), P::sy(acc_m), P::sx(acc_i), P::sy(acc_i));
+    __syncwarp();
+    if ((uint32_t)lane < n) {
+      const float4 a = meta->acc[lane];
+      const double ratio = (double)(P::init_const() / (S)hl) / (double)init_s;
+      const uint32_t hap = it.hap_start + lane;
+      const uint32_t out = it.out_x + (uint32_t)lane * it.stride;
+      S res_x, res_y = 0;
+      if (UNIFORM) {
+        res_x = uniform_gapm(b, it.read_x) * a.x + a.z;
+        if (has_y) res_y = uniform_gapm(b, it.read_y) * a.y + a.w;
+      } else {
+        res_x = a.x + a.z;
+        res_y = a.y + a.w;
+      }
+      finish(b, c, PairRef{hap, it.read_x, out}, (double)res_x * ratio);
+      if (has_y)
+        finish(b, c, PairRef{hap, it.read_y, out + (it.read_y - it.read_x)}, (double)res_y * ratio);
+    }
+    __syncwarp();
+  }
+
+  // The final log10 of one pair from its scaled likelihood `raw` (an FP32
+  // result, possibly rescaled in FP64, or an FP64 result).
+  // FP32: accepted at >= 1e-28 with an FP64 log10, else queued for FP64.
+  __device__ static void finish(const BatchView& b, const ClassLaunch& c, const PairRef& ref,
+                                double raw) {
     if (P::kSlots == 2) {
-      if (raw >= kMinAcceptedF) {
-        b.out[sl.ref.out] = log10((double)raw) - kLog10InitF;
+      if (raw >= (double)kMinAcceptedF) {
+        b.out[ref.out] = log10(raw) - kLog10InitF;
       } else {
         const uint32_t k = atomicAdd(c.rescue_count, 1u);
-        c.rescue_list[k] = sl.ref;
+        c.rescue_list[k] = ref;
       }
     } else {
       // The reference computes with flush-to-zero on (common.h:58-62), which on
       // x86 also flushes FP64 denormals: a likelihood below the normal FP64
       // range of the 2^1020 scaling becomes 0 and its log10 is -inf.  The GPU's
       // FP64 keeps denormals, so such a result is mapped to -inf here.
-      b.out[sl.ref.out] = (raw >= kDblMin) ? log10((double)raw) - kLog10InitD : -CUDART_INF;
+      b.out[ref.out] = (raw >= kDblMin) ? log10(raw) - kLog10InitD : -CUDART_INF;
     }
   }
 };
@@ -447,7 +623,7 @@ __global__ void __launch_bounds__(Forward<P, R, UNIFORM, MULTI, SAME, MINB>::kWa
   extern __shared__ uint4 smem[];
   const int lane = threadIdx.x & (kWarp - 1);
   const int warp = threadIdx.x / kWarp;
-  uint4* table = smem + warp * (TableShape<P, R, SAME>::kBytesPerWarp / 16);
+  uint4* table = smem + warp * (F::kSmemPerWarp / 16);
   const int gwarp = blockIdx.x * F::kWarpsPerBlock + warp;
   const uint32_t n = c.work_count ? *c.work_count : c.static_count;
   for (;;) {
@@ -455,7 +631,10 @@ __global__ void __launch_bounds__(Forward<P, R, UNIFORM, MULTI, SAME, MINB>::kWa
     if (lane == 0) item = atomicAdd(c.counter, 1u);
     item = __shfl_sync(kFullMask, item, 0);
     if (item >= n) break;
-    F::run_item(b, c, item, lane, gwarp, table);
+    if constexpr (F::kChain)
+      F::run_chain(b, c, item, lane, table);
+    else
+      F::run_item(b, c, item, lane, gwarp, table);
   }
 }
 

@@ -149,6 +149,49 @@ def test_edge_lengths(engine):
     assert max_err(got, ref) < TOL
 
 
+def test_chain_items_many_haps_mixed_reads(engine):
+    """Regions swept as chains: more haplotypes than one chain holds (32),
+    one-base and long haplotypes side by side, an odd read count, reads of
+    neighbouring row classes paired together, uniform and per-row gap quals in
+    one region, N bases on both sides."""
+    rng = np.random.default_rng(21)
+    regs = []
+    for nh, nr in ((70, 9), (33, 4), (32, 1), (5, 7), (1, 3)):
+        base = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, 700)]
+        haps = []
+        for k in range(nh):
+            H = int(rng.choice([1, 2, 31, 32, 33, 100, 257, 600]))
+            h = base[:H].copy()
+            mut = rng.random(H) < 0.02
+            h[mut] = np.frombuffer(b"ACGTN", np.uint8)[rng.integers(0, 5, mut.sum())]
+            haps.append(h)
+        reads, q, ins, dl, gc = [], [], [], [], []
+        for k in range(nr):
+            L = int(rng.choice([1, 31, 32, 33, 64, 65, 150, 255, 256]))
+            st = int(rng.integers(0, 700 - L))
+            r = base[st:st + L].copy()
+            if k % 3 == 0:
+                r[rng.integers(0, L)] = ord("N")
+            reads.append(r)
+            q.append(rng.integers(10, 41, L).astype(np.uint8))
+            if k % 2:
+                ins.append(rng.integers(20, 46, L).astype(np.uint8))
+                dl.append(rng.integers(20, 46, L).astype(np.uint8))
+                gc.append(rng.integers(5, 16, L).astype(np.uint8))
+            else:
+                ins.append(np.full(L, 45, np.uint8))
+                dl.append(np.full(L, 45, np.uint8))
+                gc.append(np.full(L, 10, np.uint8))
+        regs.append((haps, reads, q, ins, dl, gc))
+    b = Batch.from_regions(regs)
+    got, st = engine.batch(b, stats=True)
+    ref = oracle.batch_log10(b)
+    assert max_err(got, ref) < TOL
+    true = oracle.batch_log10(b, oracle.SCALED)
+    fin = np.isfinite(true)
+    assert np.abs(got[fin] - true[fin]).max() < CONTRACT
+
+
 def test_gap_qual_extremes(engine):
     """gcp quality 0 (gap continuation probability 1) and ins/del quality 0."""
     rng = np.random.default_rng(9)
