@@ -279,6 +279,7 @@ def run_engine(args, world, rank, local):
         cpu = None
         if not args.no_cpu_baseline:
             cpu = cpu_baseline(args)
+        stream = streaming_c5(args) if args.stream_requests > 0 else None
         line = {
             "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -318,6 +319,8 @@ def run_engine(args, world, rank, local):
             line["plain_form"] = plain
         if cpu:
             line["cpu_baseline"] = cpu
+        if stream:
+            line["streaming"] = stream
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -371,6 +374,108 @@ def plain_form(eng, args):
             "plain_launches": st["kernel_launches"]}
 
 
+def streaming_c5(args):
+    """C5: regions arrive one by one at the streaming service (rodv_service).
+
+    A pool of synthetic C5 regions (1-32 haplotypes of 100-800 bases, 1-300
+    reads of 50-250 bases) is cycled.  Saturation: requests submitted as fast
+    as two host threads can; then Poisson arrivals at fractions of that rate.
+    Per run: achieved GCUPS (cells of completed requests / wall time from the
+    first submit to the last completion) and the service's latency
+    percentiles (submit -> results available)."""
+    import ctypes
+    import threading
+    from rodv_b200 import Service, _CBatchHolder, _lib, workloads
+
+    pool_batch = workloads.make_workload("stream", seed=workloads.SEEDS["stream"],
+                                         scale=args.stream_pool / 1000.0)
+    pool = [pool_batch.subset([g]) for g in range(pool_batch.num_regions)]
+    holders = [_CBatchHolder(b) for b in pool]
+    cells = [b.cells() for b in pool]
+    sv = Service(0)
+    lib, h = sv.lib, sv.h
+
+    def run(n_req, rate):
+        """n_req requests cycling the pool; rate None = as fast as possible."""
+        tickets = [0] * n_req
+        order = np.arange(n_req) % len(pool)
+        lag = [0.0]
+
+        def submitter(k0, step):
+            t = ctypes.c_uint64()
+            for k in range(k0, n_req, step):
+                st = lib.rodv_submit_region(h, ctypes.byref(holders[order[k]].c), ctypes.byref(t))
+                if st != 0:
+                    raise RuntimeError(f"submit failed: {st}")
+                tickets[k] = t.value
+
+        def poisson():
+            rng = np.random.default_rng(17)
+            gaps = rng.exponential(1.0 / rate, n_req)
+            t_next = time.perf_counter()
+            t = ctypes.c_uint64()
+            for k in range(n_req):
+                t_next += gaps[k]
+                while True:
+                    dt = t_next - time.perf_counter()
+                    if dt <= 0:
+                        break
+                    time.sleep(dt if dt > 2e-3 else 0)
+                lag[0] = max(lag[0], time.perf_counter() - t_next)
+                st = lib.rodv_submit_region(h, ctypes.byref(holders[order[k]].c), ctypes.byref(t))
+                if st != 0:
+                    raise RuntimeError(f"submit failed: {st}")
+                tickets[k] = t.value
+
+        sv.reset_stats()
+        t0 = time.perf_counter()
+        threads = ([threading.Thread(target=submitter, args=(i, 2)) for i in range(2)]
+                   if rate is None else [threading.Thread(target=poisson)])
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+        t_sub = time.perf_counter() - t0
+        rs = _lib.RequestStats()
+        for tk in tickets:
+            st = lib.rodv_wait(h, tk, -1, None, ctypes.byref(rs))
+            if st != 0:
+                raise RuntimeError(f"request failed: {st}")
+        ss = sv.stats()
+        tot_cells = float(sum(cells[i] for i in order))
+        res = {"requests": n_req, "offered_per_s": rate,
+               "submitted_per_s": n_req / t_sub,
+               "completed_per_s": n_req / (ss["wall_ms"] / 1e3),
+               "gcups": tot_cells / (ss["wall_ms"] / 1e3) / 1e9,
+               "device_gcups": tot_cells / (ss["device_ms"] / 1e3) / 1e9,
+               "p50_ms": ss["latency_p50_ms"], "p99_ms": ss["latency_p99_ms"],
+               "max_ms": ss["latency_max_ms"], "batches": ss["batches"],
+               "mean_batch_regions": ss["mean_batch_regions"],
+               "host_launch_ms": ss["host_launch_ms"], "host_finish_ms": ss["host_finish_ms"],
+               "wall_ms": ss["wall_ms"], "device_ms": ss["device_ms"],
+               "fp64_pairs": ss["fp64_pairs"]}
+        if rate is not None:
+            res["max_submit_lag_ms"] = lag[0] * 1e3
+        return res
+
+    run(len(pool), None)  # warm-up (buffers grow to size)
+    sat = run(args.stream_requests, None)
+    sat_rate = sat["completed_per_s"]
+    runs = []
+    for frac in (0.25, 0.5, 0.75, 0.9):
+        rate = frac * sat_rate
+        n = max(50, int(rate * args.stream_seconds))
+        r = run(n, rate)
+        r["fraction_of_saturation"] = frac
+        runs.append(r)
+    sv.close()
+    mean_cells = float(np.mean(cells))
+    return {"config": "C5 streaming: Poisson arrivals; per region 1-32 haplotypes of 100-800 "
+                      "bases, 1-300 reads of 50-250 bases (synthetic, seeded)",
+            "pool_regions": len(pool), "mean_cells_per_region": mean_cells,
+            "saturation": sat, "saturation_regions_per_s": sat_rate, "poisson": runs}
+
+
 def cpu_baseline(args):
     import oracle
     if not oracle.ref_available():
@@ -392,8 +497,9 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["rodv", "reference"], default="rodv")
-    ap.add_argument("--mode", choices=["bench", "profile"], default="bench",
-                    help="profile: resident steps only, for ncu captures")
+    ap.add_argument("--mode", choices=["bench", "profile", "streaming"], default="bench",
+                    help="profile: resident steps only, for ncu captures; streaming: the C5 "
+                         "service measurement only")
     ap.add_argument("--workload", default="uneven")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--e2e-steps", type=int, default=3)
@@ -404,10 +510,18 @@ def main():
                     help="reference arm: wall seconds of CPU work per step")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="cpu_baseline: wall seconds of CPU work")
+    ap.add_argument("--stream-pool", type=int, default=300,
+                    help="streaming (C5): regions in the cycled pool")
+    ap.add_argument("--stream-requests", type=int, default=1200,
+                    help="streaming (C5): requests of the saturation run (0: skip C5)")
+    ap.add_argument("--stream-seconds", type=float, default=3.0,
+                    help="streaming (C5): seconds of arrivals per Poisson rate")
     args = ap.parse_args()
     world, rank, local = dist_env()
     if args.mode == "profile":
         run_profile(args, local)
+    elif args.mode == "streaming":
+        print(json.dumps({"mode": "streaming", "streaming": streaming_c5(args)}), flush=True)
     elif args.impl == "reference":
         run_reference(args, world, rank)
     else:

@@ -47,7 +47,8 @@ enum {
   RODV_ERR_ADMISSION = 9,     /* streaming: region does not fit the device memory budget */
   RODV_ERR_NOT_FOUND = 10,    /* streaming: unknown ticket */
   RODV_ERR_NOT_READY = 11,    /* streaming: result not yet available */
-  RODV_ERR_SHUTDOWN = 12      /* streaming: service stopped */
+  RODV_ERR_SHUTDOWN = 12,     /* streaming: service stopped */
+  RODV_ERR_INTERNAL = 13      /* an internal consistency check failed (a bug; please report) */
 };
 
 /* Engine limits (inputs beyond them are rejected with RODV_ERR_TOO_LONG). */
@@ -205,6 +206,72 @@ rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32_t use_doub
 #define RODV_TUNE_CLASSES 18
 rodv_status rodv_autotune(rodv_engine* engine, const char* cache_path, int32_t force,
                           int32_t* variants_out);
+
+/* ---- Streaming service -----------------------------------------------------
+ * No single counterpart in the reference: it stands for a caller that runs
+ * schedule_pairhmm (pairhmm_schedule.cpp:116-340) once per region as regions
+ * arrive.  rodv_submit_region copies one or more regions (a rodv_batch; the
+ * caller's buffers may be reused as soon as it returns) into the service's
+ * queue and returns a ticket.  A worker thread puts everything submitted while
+ * the GPU was busy into the next device batch (continuous batching over two
+ * streams: the next batch is packed and uploaded while the current one
+ * computes).  A region's results are bitwise identical whatever it was
+ * batched with.
+ * Admission: opts->device_memory_budget bytes (0 = half of the free device
+ * memory) are split between the two batch slots; a request that cannot fit
+ * one slot is refused with RODV_ERR_ADMISSION; rodv_submit_region blocks while
+ * opts->max_inflight requests (0 = 4096) are queued or computing.
+ * rodv_poll returns RODV_ERR_NOT_READY until the results are available, then
+ * copies them (hap-major per region, regions in submission order, as
+ * rodv_pairhmm_batch writes them) and forgets the ticket; a later call returns
+ * RODV_ERR_NOT_FOUND.  rodv_wait blocks up to timeout_ms (< 0: no limit).
+ * A request whose batch failed returns that failure's status.
+ * rodv_service_destroy finishes all submitted work, then stops. */
+typedef struct rodv_service rodv_service;
+
+typedef struct rodv_request_stats {
+  uint64_t pairs;
+  uint64_t cells;
+  uint64_t fp64_pairs;          /* pairs of the request's device batch computed in FP64 */
+  uint64_t batch_id;            /* device batch the request was computed in */
+  uint32_t batch_regions;       /* regions in that batch */
+  uint32_t pad_;
+  double queue_ms;              /* submit -> its batch started packing */
+  double latency_ms;            /* submit -> results available */
+} rodv_request_stats;
+
+typedef struct rodv_service_stats {
+  uint64_t submitted;           /* requests since the last reset */
+  uint64_t completed;
+  uint64_t failed;
+  uint64_t batches;
+  uint64_t regions;
+  uint64_t pairs;
+  uint64_t cells;
+  uint64_t fp64_pairs;
+  double latency_p50_ms;        /* over completed requests (nearest rank) */
+  double latency_p99_ms;
+  double latency_max_ms;
+  double latency_mean_ms;
+  double device_ms;             /* sum of the batches' kernel times */
+  double wall_ms;               /* first submit -> last completion */
+  double mean_batch_regions;
+  double host_launch_ms;        /* worker time forming, packing and enqueueing batches */
+  double host_finish_ms;        /* worker time handing results to requests */
+} rodv_service_stats;
+
+rodv_status rodv_service_create(const rodv_options* opts, rodv_service** out);
+void rodv_service_destroy(rodv_service* service);
+rodv_status rodv_submit_region(rodv_service* service, const rodv_batch* regions,
+                               uint64_t* ticket);
+rodv_status rodv_poll(rodv_service* service, uint64_t ticket, double* out_log10,
+                      rodv_request_stats* stats);
+rodv_status rodv_wait(rodv_service* service, uint64_t ticket, int32_t timeout_ms,
+                      double* out_log10, rodv_request_stats* stats);
+rodv_status rodv_service_get_stats(rodv_service* service, rodv_service_stats* out);
+void rodv_service_reset_stats(rodv_service* service);
+/* Details of the service's last failure (valid until this thread's next call). */
+const char* rodv_service_last_error(rodv_service* service);
 
 /* Human-readable name of a status code (static storage). */
 const char* rodv_status_string(rodv_status status);

@@ -11,6 +11,8 @@ module is a thin ctypes layer over it that mirrors roDV's own interface:
   (src/core/pairhmm/intra/pairhmm_api.h:17-20): one pair.
 * :class:`Engine` -- batches of many regions (:class:`Batch`), device-resident
   batches, the plain one-pair-per-launch form, and the peak measurement.
+* :class:`Service` -- the streaming service: regions submitted as they come,
+  continuously batched on the device, results by ticket, latency statistics.
 """
 from __future__ import annotations
 
@@ -24,7 +26,7 @@ from . import _lib
 from ._lib import RodvError
 from .batch import Batch
 
-__all__ = ["Engine", "DeviceBatch", "Batch", "RodvError", "schedule_pairhmm",
+__all__ = ["Engine", "DeviceBatch", "Service", "Batch", "RodvError", "schedule_pairhmm",
            "compute_likelihoods", "TestCase", "default_engine"]
 
 
@@ -177,6 +179,97 @@ class Engine:
         self._check(self.lib.rodv_measure_peaks(self.h, *[ctypes.byref(x) for x in v]))
         return {"fp32_gflops": v[0].value, "fp32x2_gflops": v[1].value,
                 "fp64_gflops": v[2].value, "sm_mhz": v[3].value}
+
+
+class Service:
+    """The streaming service (rodv_service): submit regions at any time, get
+    each request's results by ticket.  Requests are batched continuously on
+    the device; a region's results do not depend on what it was batched
+    with."""
+
+    def __init__(self, device: int = 0, force_fp64: bool = False, verbose: bool = False,
+                 device_memory_budget: int = 0, max_inflight: int = 0, autotune: int = 0,
+                 tune_cache: Optional[str] = None):
+        self.lib = _lib.load()
+        opts = _lib.Options()
+        self.lib.rodv_default_options(ctypes.byref(opts))
+        opts.device = device
+        opts.force_fp64 = int(force_fp64)
+        opts.verbose = int(verbose)
+        opts.device_memory_budget = device_memory_budget
+        opts.max_inflight = max_inflight
+        opts.autotune = autotune
+        self._tune_cache = tune_cache.encode() if tune_cache else None
+        opts.tune_cache = self._tune_cache
+        h = ctypes.c_void_p()
+        st = self.lib.rodv_service_create(ctypes.byref(opts), ctypes.byref(h))
+        if st != _lib.RODV_OK:
+            detail = self.lib.rodv_last_error(None) or b""
+            raise RodvError(st, "service creation failed: " + detail.decode(errors="replace"))
+        self.h = h
+        self._pairs = {}
+        self._lock = threading.Lock()
+
+    def close(self) -> None:
+        """Finishes all submitted work, then stops the service."""
+        if getattr(self, "h", None):
+            self.lib.rodv_service_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int) -> None:
+        if st != _lib.RODV_OK:
+            detail = self.lib.rodv_service_last_error(self.h) if self.h else b""
+            raise RodvError(st, detail.decode(errors="replace") if detail else "")
+
+    def submit(self, b: Batch) -> int:
+        """Queues the regions of ``b``; returns the request's ticket."""
+        holder = _CBatchHolder(b)
+        t = ctypes.c_uint64()
+        self._check(self.lib.rodv_submit_region(self.h, ctypes.byref(holder.c), ctypes.byref(t)))
+        with self._lock:
+            self._pairs[t.value] = b.num_pairs
+        return t.value
+
+    def _result(self, ticket: int, timeout_ms: Optional[int], stats: bool):
+        with self._lock:
+            n = self._pairs.get(ticket)
+        out = np.empty(n if n is not None else 0, dtype=np.float64)
+        rs = _lib.RequestStats()
+        optr = _ptr(out, _lib._f64p) if n else None
+        if timeout_ms == 0:
+            st = self.lib.rodv_poll(self.h, ticket, optr, ctypes.byref(rs))
+        else:
+            st = self.lib.rodv_wait(self.h, ticket, -1 if timeout_ms is None else timeout_ms, optr,
+                                    ctypes.byref(rs))
+        if st == _lib.RODV_ERR_NOT_READY:
+            return None
+        if st != _lib.RODV_ERR_NOT_FOUND:
+            with self._lock:
+                self._pairs.pop(ticket, None)
+        self._check(st)
+        return (out, rs.as_dict()) if stats else out
+
+    def poll(self, ticket: int, stats: bool = False):
+        """The request's results (flat, hap-major per region), or None if not ready."""
+        return self._result(ticket, 0, stats)
+
+    def wait(self, ticket: int, timeout_ms: Optional[int] = None, stats: bool = False):
+        """Blocks until the request is done; None if timeout_ms passes first."""
+        return self._result(ticket, timeout_ms, stats)
+
+    def stats(self) -> dict:
+        ss = _lib.ServiceStats()
+        self._check(self.lib.rodv_service_get_stats(self.h, ctypes.byref(ss)))
+        return ss.as_dict()
+
+    def reset_stats(self) -> None:
+        self.lib.rodv_service_reset_stats(self.h)
 
 
 _default: Optional[Engine] = None

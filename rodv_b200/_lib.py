@@ -12,11 +12,14 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "librodv_pairhmm.so")
 
 RODV_OK = 0
+RODV_ERR_NOT_FOUND = 10
+RODV_ERR_NOT_READY = 11
 STATUS_NAMES = {
     0: "RODV_OK", 1: "RODV_ERR_INVALID_ARG", 2: "RODV_ERR_EMPTY", 3: "RODV_ERR_INVALID_BASE",
     4: "RODV_ERR_NO_DEVICE", 5: "RODV_ERR_CUDA", 6: "RODV_ERR_OUT_OF_MEMORY",
     7: "RODV_ERR_TOO_LONG", 8: "RODV_ERR_DEVICE_CHECK", 9: "RODV_ERR_ADMISSION",
     10: "RODV_ERR_NOT_FOUND", 11: "RODV_ERR_NOT_READY", 12: "RODV_ERR_SHUTDOWN",
+    13: "RODV_ERR_INTERNAL",
 }
 
 
@@ -66,6 +69,31 @@ class Stats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "pad_"}
 
 
+class RequestStats(ctypes.Structure):
+    _fields_ = [("pairs", ctypes.c_uint64), ("cells", ctypes.c_uint64),
+                ("fp64_pairs", ctypes.c_uint64), ("batch_id", ctypes.c_uint64),
+                ("batch_regions", ctypes.c_uint32), ("pad_", ctypes.c_uint32),
+                ("queue_ms", ctypes.c_double), ("latency_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "pad_"}
+
+
+class ServiceStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64),
+                ("failed", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("regions", ctypes.c_uint64), ("pairs", ctypes.c_uint64),
+                ("cells", ctypes.c_uint64), ("fp64_pairs", ctypes.c_uint64),
+                ("latency_p50_ms", ctypes.c_double), ("latency_p99_ms", ctypes.c_double),
+                ("latency_max_ms", ctypes.c_double), ("latency_mean_ms", ctypes.c_double),
+                ("device_ms", ctypes.c_double), ("wall_ms", ctypes.c_double),
+                ("mean_batch_regions", ctypes.c_double), ("host_launch_ms", ctypes.c_double),
+                ("host_finish_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 # (name, restype, argtypes) of every function declared in include/rodv_pairhmm.h
 SIGNATURES = [
     ("rodv_default_options", None, [ctypes.POINTER(Options)]),
@@ -91,6 +119,18 @@ SIGNATURES = [
                                                     ctypes.c_void_p, ctypes.c_void_p]),
     ("rodv_autotune", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int32,
                                        ctypes.POINTER(ctypes.c_int32)]),
+    ("rodv_service_create", ctypes.c_int32, [ctypes.POINTER(Options),
+                                             ctypes.POINTER(ctypes.c_void_p)]),
+    ("rodv_service_destroy", None, [ctypes.c_void_p]),
+    ("rodv_submit_region", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(CBatch), _u64p]),
+    ("rodv_poll", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, _f64p,
+                                   ctypes.POINTER(RequestStats)]),
+    ("rodv_wait", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32, _f64p,
+                                   ctypes.POINTER(RequestStats)]),
+    ("rodv_service_get_stats", ctypes.c_int32, [ctypes.c_void_p,
+                                                ctypes.POINTER(ServiceStats)]),
+    ("rodv_service_reset_stats", None, [ctypes.c_void_p]),
+    ("rodv_service_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
     ("rodv_status_string", ctypes.c_char_p, [ctypes.c_int32]),
     ("rodv_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
 ]

@@ -5,8 +5,10 @@
 #include <string>
 
 #include "engine.h"
+#include "service.h"
 
 using rodv::Engine;
+using rodv::Service;
 
 static_assert(RODV_TUNE_CLASSES == rodv::kNumClasses, "tuning classes out of sync");
 
@@ -172,6 +174,7 @@ const char* rodv_status_string(rodv_status s) {
     case RODV_ERR_NOT_FOUND: return "unknown ticket";
     case RODV_ERR_NOT_READY: return "result not ready";
     case RODV_ERR_SHUTDOWN: return "service stopped";
+    case RODV_ERR_INTERNAL: return "internal consistency check failed";
     default: return "unknown status";
   }
 }
@@ -182,6 +185,71 @@ const char* rodv_last_error(rodv_engine* engine) {
     return g_create_error.c_str();
   }
   return engine->impl->last_error();
+}
+
+// ---- streaming service ----------------------------------------------------
+rodv_status rodv_service_create(const rodv_options* opts, rodv_service** out) {
+  if (!out) return RODV_ERR_INVALID_ARG;
+  *out = nullptr;
+  rodv_options o;
+  rodv_default_options(&o);
+  if (opts) o = *opts;
+  Service* sv = new (std::nothrow) Service(o);
+  if (!sv) return RODV_ERR_OUT_OF_MEMORY;
+  const rodv_status s = sv->init();
+  if (s != RODV_OK) {
+    {
+      std::lock_guard<std::mutex> lk(g_create_mu);
+      g_create_error = sv->last_error();
+    }
+    delete sv;
+    return s;
+  }
+  *out = new (std::nothrow) rodv_service{sv};
+  if (!*out) {
+    delete sv;
+    return RODV_ERR_OUT_OF_MEMORY;
+  }
+  return RODV_OK;
+}
+
+void rodv_service_destroy(rodv_service* service) {
+  if (!service) return;
+  delete service->impl;
+  delete service;
+}
+
+rodv_status rodv_submit_region(rodv_service* service, const rodv_batch* regions,
+                               uint64_t* ticket) {
+  if (!service || !regions || !ticket) return RODV_ERR_INVALID_ARG;
+  return service->impl->submit(*regions, ticket);
+}
+
+rodv_status rodv_poll(rodv_service* service, uint64_t ticket, double* out_log10,
+                      rodv_request_stats* stats) {
+  if (!service) return RODV_ERR_INVALID_ARG;
+  return service->impl->result(ticket, 0, out_log10, stats);
+}
+
+rodv_status rodv_wait(rodv_service* service, uint64_t ticket, int32_t timeout_ms,
+                      double* out_log10, rodv_request_stats* stats) {
+  if (!service) return RODV_ERR_INVALID_ARG;
+  return service->impl->result(ticket, timeout_ms, out_log10, stats);
+}
+
+rodv_status rodv_service_get_stats(rodv_service* service, rodv_service_stats* out) {
+  if (!service) return RODV_ERR_INVALID_ARG;
+  return service->impl->stats(out);
+}
+
+void rodv_service_reset_stats(rodv_service* service) {
+  if (service) service->impl->reset_stats();
+}
+
+const char* rodv_service_last_error(rodv_service* service) {
+  static thread_local std::string msg;
+  msg = service ? service->impl->last_error() : std::string();
+  return msg.c_str();
 }
 
 }  // extern "C"

@@ -232,29 +232,64 @@ int Engine::persistent_blocks(const KernelInfo& k) const {
 // ---------------------------------------------------------------------------
 // Packing
 // ---------------------------------------------------------------------------
+rodv_status validate_batch(const rodv_batch& b, bool check_bases, uint64_t* num_pairs,
+                           std::string* msg) {
+  auto bad = [&](rodv_status st, const std::string& m) {
+    if (msg) *msg = m;
+    return st;
+  };
+  if (b.num_regions == 0 || !b.regions) return bad(RODV_ERR_EMPTY, "batch has no regions");
+  if (!b.hap_bases || !b.hap_offsets || !b.hap_lengths || !b.read_bases || !b.base_quals ||
+      !b.ins_quals || !b.del_quals || !b.gcp_quals || !b.read_offsets || !b.read_lengths)
+    return bad(RODV_ERR_INVALID_ARG, "null array in batch");
+  uint64_t pairs = 0;
+  for (uint32_t g = 0; g < b.num_regions; ++g) {
+    const rodv_region& r = b.regions[g];
+    if (r.num_haps == 0 || r.num_reads == 0)
+      return bad(RODV_ERR_EMPTY, "region " + std::to_string(g) + " has no haplotypes or reads");
+    if ((uint64_t)r.hap_start + r.num_haps > b.num_haps ||
+        (uint64_t)r.read_start + r.num_reads > b.num_reads)
+      return bad(RODV_ERR_INVALID_ARG, "region " + std::to_string(g) + " indexes out of range");
+    pairs += (uint64_t)r.num_haps * r.num_reads;
+  }
+  if (pairs >= 0xffffffffull) return bad(RODV_ERR_TOO_LONG, "batch has 2^32 or more pairs");
+  for (uint32_t h = 0; h < b.num_haps; ++h) {
+    const uint32_t len = b.hap_lengths[h];
+    if (len == 0) return bad(RODV_ERR_INVALID_ARG, "haplotype " + std::to_string(h) + " is empty");
+    if (len > RODV_MAX_HAP_LEN) return bad(RODV_ERR_TOO_LONG, "haplotype longer than limit");
+    if (check_bases)
+      for (uint32_t k = 0; k < len; ++k)
+        if (kCodes.v[b.hap_bases[b.hap_offsets[h] + k]] == 0xff)
+          return bad(RODV_ERR_INVALID_BASE, "haplotype base is not one of A, C, G, T, N");
+  }
+  for (uint32_t r = 0; r < b.num_reads; ++r) {
+    const uint32_t len = b.read_lengths[r];
+    if (len == 0) return bad(RODV_ERR_INVALID_ARG, "read " + std::to_string(r) + " is empty");
+    if (len > RODV_MAX_READ_LEN) return bad(RODV_ERR_TOO_LONG, "read longer than limit");
+    if (check_bases)
+      for (uint32_t k = 0; k < len; ++k)
+        if (kCodes.v[b.read_bases[b.read_offsets[r] + k]] == 0xff)
+          return bad(RODV_ERR_INVALID_BASE, "read base is not one of A, C, G, T, N");
+  }
+  if (num_pairs) *num_pairs = pairs;
+  return RODV_OK;
+}
+
 rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64) {
   plan = PackedPlan{};
   plan.fp64 = fp64;
-  if (b.num_regions == 0 || !b.regions) return fail(RODV_ERR_EMPTY, "batch has no regions");
-  if (!b.hap_bases || !b.hap_offsets || !b.hap_lengths || !b.read_bases || !b.base_quals ||
-      !b.ins_quals || !b.del_quals || !b.gcp_quals || !b.read_offsets || !b.read_lengths)
-    return fail(RODV_ERR_INVALID_ARG, "null array in batch");
-  const uint32_t G = b.num_regions;
   uint64_t pairs = 0;
-  for (uint32_t g = 0; g < G; ++g) {
-    const rodv_region& r = b.regions[g];
-    if (r.num_haps == 0 || r.num_reads == 0)
-      return fail(RODV_ERR_EMPTY, "region " + std::to_string(g) + " has no haplotypes or reads");
-    if ((uint64_t)r.hap_start + r.num_haps > b.num_haps ||
-        (uint64_t)r.read_start + r.num_reads > b.num_reads)
-      return fail(RODV_ERR_INVALID_ARG, "region " + std::to_string(g) + " indexes out of range");
-    pairs += (uint64_t)r.num_haps * r.num_reads;
+  {
+    std::string msg;
+    const rodv_status vs = validate_batch(b, false, &pairs, &msg);
+    if (vs != RODV_OK) return fail(vs, msg);
   }
-  if (pairs >= 0xffffffffull) return fail(RODV_ERR_TOO_LONG, "batch has 2^32 or more pairs");
+  const uint32_t G = b.num_regions;
   plan.num_pairs = pairs;
   plan.num_haps = b.num_haps;
   plan.num_reads = b.num_reads;
   plan.regions.assign(b.regions, b.regions + G);
+  plan.hap_len.assign(b.hap_lengths, b.hap_lengths + b.num_haps);
 
   // haplotype code buffer: [pad][hap 0][sep][hap 1][sep]...[hap n-1][sep]
   // [pad + max len + pad]; any run of consecutive haplotypes is one chain.
@@ -333,12 +368,25 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   std::vector<uint32_t> chains((size_t)G * K, 0);  // chain items of class c in region g
   std::vector<uint64_t> cpairs((size_t)G * K, 0);  // pairs those chains compute
   std::vector<uint64_t> hsum(G, 0);
+  std::vector<uint32_t> hmax(G, 0);
+  // multi-pass leftovers: the last read of each multi-pass class in the region
+  std::vector<uint32_t> left_read((size_t)G * 2, kNoPair);
   parallel_for(G, 64, [&](size_t lo, size_t hi) {
     std::vector<uint32_t> sr;
     for (size_t g = lo; g < hi; ++g) {
       const rodv_region& rg = b.regions[g];
-      for (uint32_t r = 0; r < rg.num_reads; ++r) rc[g * K + read_class[rg.read_start + r]]++;
-      for (uint32_t h = 0; h < rg.num_haps; ++h) hsum[g] += b.hap_lengths[rg.hap_start + h];
+      for (uint32_t r = 0; r < rg.num_reads; ++r) {
+        const uint32_t read = rg.read_start + r;
+        const int c = read_class[read];
+        rc[g * K + c]++;
+        if (class_multi(c)) left_read[g * 2 + (c - kSinglePassClasses)] = read;
+      }
+      for (int u = 0; u < 2; ++u)
+        if (!(rc[g * K + kSinglePassClasses + u] & 1)) left_read[g * 2 + u] = kNoPair;
+      for (uint32_t h = 0; h < rg.num_haps; ++h) {
+        hsum[g] += b.hap_lengths[rg.hap_start + h];
+        hmax[g] = std::max(hmax[g], b.hap_lengths[rg.hap_start + h]);
+      }
       if (fp64) continue;
       sorted_single(rg, sr);
       for (size_t k = 0; k < sr.size(); k += 2) {
@@ -399,12 +447,26 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       }
     }
   }
+  // Multi-pass leftovers are paired only with leftovers of the same pass
+  // count (a partner with more passes would send this read's last row
+  // through pass-through rows and change its rounding), so a pair's result
+  // does not depend on the rest of the batch.
+  auto passes_of = [&](uint32_t read) { return (b.read_lengths[read] + kPassRows - 1) / kPassRows; };
+  std::vector<uint64_t> left_by_passes[2];
+  for (int u = 0; u < 2; ++u) left_by_passes[u].assign(RODV_MAX_READ_LEN / kPassRows + 2, 0);
+  for (uint32_t g = 0; g < G; ++g)
+    for (int u = 0; u < 2; ++u)
+      if (left_read[g * 2 + u] != kNoPair)
+        left_by_passes[u][passes_of(left_read[g * 2 + u])] += b.regions[g].num_haps;
   for (int c = 0; c < kNumClasses; ++c) {
     // FP64 list capacity: every pair whose FP32 work is in class c (or, FP64
     // forced, every pair whose read is of class c)
     plan.pairs[c] = (uint32_t)(fp64 ? list_tot[c] : cap_tot[c]);
     plan.same_items[c] = fp64 ? 0u : (uint32_t)same_tot[c];
-    plan.diff_items[c] = fp64 ? 0u : (uint32_t)((left_tot[c] + 1) / 2);
+    uint64_t diff = 0;
+    if (class_multi(c))
+      for (uint64_t n : left_by_passes[c - kSinglePassClasses]) diff += (n + 1) / 2;
+    plan.diff_items[c] = fp64 ? 0u : (uint32_t)diff;
   }
   for (uint32_t g = 0; g < G; ++g) {
     const rodv_region& rg = b.regions[g];
@@ -543,7 +605,8 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
           const uint32_t cap = plan.chain_haps[c];
           for (uint32_t h0 = 0; h0 < rg.num_haps; h0 += cap)
             ci[next[c]++] = ChainItem{rg.hap_start + h0, std::min(cap, rg.num_haps - h0), sr[k],
-                                      two ? sr[k + 1] : kNoPair, out_of(h0, sr[k]), N};
+                                      two ? sr[k + 1] : kNoPair, out_of(h0, sr[k]), N, hmax[g],
+                                      0};
         }
       }
       for (auto& v : byclass) v.clear();
@@ -569,17 +632,26 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
     }
   });
   if (!fp64) {
-    // leftovers: sorted by haplotype length, paired longest-first
-    for (int c = 0; c < kNumClasses; ++c) {
+    // leftovers: grouped by pass count, sorted by haplotype length within a
+    // group, paired longest-first within the group
+    for (int c = kSinglePassClasses; c < kNumClasses; ++c) {
       std::vector<PairRef>& lv = leftovers[c];
       std::stable_sort(lv.begin(), lv.end(), [&](const PairRef& x, const PairRef& y) {
+        const uint32_t px = passes_of(x.read), py = passes_of(y.read);
+        if (px != py) return px > py;
         return b.hap_lengths[x.hap] > b.hap_lengths[y.hap];
       });
       DiffItem* di = reinterpret_cast<DiffItem*>(s + plan.off_diff[c]);
-      for (size_t k = 0; k < plan.diff_items[c]; ++k) {
-        di[k].x = lv[2 * k];
-        di[k].y = (2 * k + 1 < lv.size()) ? lv[2 * k + 1] : PairRef{0, kNoPair, 0};
+      size_t n = 0;
+      for (size_t k = 0; k < lv.size();) {
+        const bool two = k + 1 < lv.size() && passes_of(lv[k].read) == passes_of(lv[k + 1].read);
+        di[n].x = lv[k];
+        di[n].y = two ? lv[k + 1] : PairRef{0, kNoPair, 0};
+        ++n;
+        k += two ? 2 : 1;
       }
+      if (n != plan.diff_items[c])
+        return fail(RODV_ERR_INTERNAL, "leftover pairing count mismatch");
     }
   }
   // cells
@@ -598,7 +670,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
 // Launches
 // ---------------------------------------------------------------------------
 rodv_status Engine::launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, int c, bool same,
-                                      int variant, int blocks_cap) {
+                                      int variant, int blocks_cap, cudaStream_t stream) {
   ArenaView a = arena_view(plan, dbase, tab_);
   const uint32_t n = same ? plan.same_items[c] : plan.diff_items[c];
   if (!n) return RODV_OK;
@@ -618,32 +690,32 @@ rodv_status Engine::launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, in
   int blocks = std::max(1, std::min(persistent_blocks(k), need));
   if (blocks_cap > 0) blocks = std::min(blocks, blocks_cap);
   void* args[] = {&a.view, &cl};
-  RODV_CUDA(cudaLaunchKernel(k.fn, dim3(blocks), dim3(k.threads), args, k.smem_bytes, stream_));
+  RODV_CUDA(cudaLaunchKernel(k.fn, dim3(blocks), dim3(k.threads), args, k.smem_bytes, stream));
   return RODV_OK;
 }
 
 rodv_status Engine::launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stats* st,
-                               bool timed, bool split, int parts) {
+                               cudaStream_t stream, cudaEvent_t* ev, int parts) {
   ArenaView a = arena_view(plan, dbase, tab_);
   uint32_t launches = 0;
   if (parts & 1) {
-    RODV_CUDA(cudaMemsetAsync(a.counts, 0, kCountWords * 4, stream_));
+    RODV_CUDA(cudaMemsetAsync(a.counts, 0, kCountWords * 4, stream));
     if (plan.fp64)  // every pair goes to the FP64 kernels: the uploaded lists are full
       RODV_CUDA(cudaMemcpyAsync(a.counts + kCtrRescue, dbase + plan.off_preset,
-                                kNumClasses * 4, cudaMemcpyDeviceToDevice, stream_));
+                                kNumClasses * 4, cudaMemcpyDeviceToDevice, stream));
   }
-  if (timed) RODV_CUDA(cudaEventRecord(ev_[0], stream_));
+  if (ev) RODV_CUDA(cudaEventRecord(ev[0], stream));
   if (!plan.fp64 && (parts & 1)) {
     for (int c = 0; c < kNumClasses; ++c) {
       for (int same = 1; same >= 0; --same) {
         if (!(same ? plan.same_items[c] : plan.diff_items[c])) continue;
-        rodv_status s = launch_fp32_class(plan, dbase, c, same != 0, variant_[c], 0);
+        rodv_status s = launch_fp32_class(plan, dbase, c, same != 0, variant_[c], 0, stream);
         if (s != RODV_OK) return s;
         ++launches;
       }
     }
   }
-  if (timed || split) RODV_CUDA(cudaEventRecord(ev_[1], stream_));
+  if (ev) RODV_CUDA(cudaEventRecord(ev[1], stream));
   for (int c = 0; c < kNumClasses && (parts & 2); ++c) {
     if (!plan.pairs[c]) continue;
     const KernelInfo k =
@@ -659,10 +731,10 @@ rodv_status Engine::launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stat
     const int need = (int)((plan.pairs[c] + k.warps_per_block - 1) / k.warps_per_block);
     const int blocks = std::max(1, std::min(persistent_blocks(k), need));
     void* args[] = {&a.view, &cl};
-    RODV_CUDA(cudaLaunchKernel(k.fn, dim3(blocks), dim3(k.threads), args, k.smem_bytes, stream_));
+    RODV_CUDA(cudaLaunchKernel(k.fn, dim3(blocks), dim3(k.threads), args, k.smem_bytes, stream));
     ++launches;
   }
-  if (timed) RODV_CUDA(cudaEventRecord(ev_[2], stream_));
+  if (ev) RODV_CUDA(cudaEventRecord(ev[2], stream));
   if (st) st->kernel_launches += launches;
   return RODV_OK;
 }
@@ -696,7 +768,7 @@ rodv_status Engine::run_host(const rodv_batch& b, double* out, rodv_stats* st, b
   uint8_t* d = static_cast<uint8_t*>(arena_.ptr);
   RODV_CUDA(cudaEventRecord(ev_[3], stream_));
   RODV_CUDA(cudaMemcpyAsync(d, staging_.ptr, plan.upload_bytes, cudaMemcpyHostToDevice, stream_));
-  s = launch_all(plan, d, st, true, true, 3);
+  s = launch_all(plan, d, st, stream_, ev_, 3);
   if (s != RODV_OK) return s;
   uint8_t* hs = static_cast<uint8_t*>(out_staging_.ptr);
   RODV_CUDA(cudaMemcpyAsync(hs, d + plan.off_out, plan.num_pairs * 8, cudaMemcpyDeviceToHost,
@@ -758,7 +830,7 @@ rodv_status Engine::run_device(rodv_device_batch* db, rodv_stats* st) {
     for (int part = 0; part < 2; ++part) {
       rodv_stats cap{};
       RODV_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-      rodv_status s = launch_all(db->plan, d, &cap, false, false, part == 0 ? 1 : 2);
+      rodv_status s = launch_all(db->plan, d, &cap, stream_, nullptr, part == 0 ? 1 : 2);
       cudaGraph_t g = nullptr;
       const cudaError_t ce = cudaStreamEndCapture(stream_, &g);
       if (s != RODV_OK) {
@@ -836,7 +908,8 @@ rodv_status Engine::plain(rodv_device_batch* db, double* out, rodv_stats* st) {
           const SameItem item{rg.hap_start + h, read, kNoPair, (uint32_t)p};
           std::memcpy(hw, &item, sizeof(item));
         } else {
-          const ChainItem item{rg.hap_start + h, 1, read, kNoPair, (uint32_t)p, 0};
+          const ChainItem item{rg.hap_start + h, 1, read, kNoPair, (uint32_t)p, 0,
+                               plan.hap_len[rg.hap_start + h], 0};
           std::memcpy(hw, &item, sizeof(item));
         }
         const PairRef ref{rg.hap_start + h, read, (uint32_t)p};
@@ -993,7 +1066,7 @@ rodv_status Engine::autotune(const char* cache_path, int force, int32_t* variant
       for (int rep = 0; rep < 3; ++rep) {
         RODV_CUDA(cudaMemsetAsync((void*)counts, 0, kCountWords * 4, stream_));
         RODV_CUDA(cudaEventRecord(ev_[0], stream_));
-        s = launch_fp32_class(db->plan, d, c, true, v, 0);
+        s = launch_fp32_class(db->plan, d, c, true, v, 0, stream_);
         if (s != RODV_OK) {
           delete db;
           return s;

@@ -83,10 +83,20 @@ struct PackedPlan {
   uint32_t scratch_cols = 0;
   // host copies kept for the plain per-pair form
   std::vector<rodv_region> regions;
+  std::vector<uint32_t> hap_len;
   std::vector<uint8_t> read_class;
 };
 
+// Checks a batch's regions, lengths, limits and (check_bases) every base;
+// the status and message the engine would fail the batch with.
+rodv_status validate_batch(const rodv_batch& b, bool check_bases, uint64_t* num_pairs,
+                           std::string* msg);
+
+class Service;
+
 class Engine {
+  friend class Service;
+
  public:
   explicit Engine(const rodv_options& opt);
   ~Engine();
@@ -107,10 +117,13 @@ class Engine {
 
  private:
   rodv_status pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64);
-  rodv_status launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stats* st, bool timed,
-                         bool split, int parts);
+  // parts: 1 = counter reset and FP32 launches, 2 = FP64 launches.  ev: null,
+  // or three events recorded before the FP32 launches, between the two parts
+  // and after the FP64 launches.
+  rodv_status launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stats* st,
+                         cudaStream_t stream, cudaEvent_t* ev, int parts);
   rodv_status launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, int cls, bool same,
-                                int variant, int blocks_cap);
+                                int variant, int blocks_cap, cudaStream_t stream);
   rodv_status check_errors(const PackedPlan& plan, uint8_t* dbase);
   int persistent_blocks(const KernelInfo& k) const;
   std::string device_key() const;

@@ -80,17 +80,22 @@ struct SameItem {
   uint32_t out_x;
 };
 
-// Two reads of one region against every haplotype of the region, swept in
-// one pass over the concatenated haplotype columns.  The result of
-// (haplotype hap_start + i, read_x) goes to out_x + i * stride; read_y's to
-// that index + (read_y - read_x).  read_y may be kNoPair.
-struct ChainItem {
+// Two reads of one region against consecutive haplotypes of the region
+// (up to kChainHaps), swept in one pass over their concatenated columns.  The
+// result of (haplotype hap_start + i, read_x) goes to out_x + i * stride;
+// read_y's to that index + (read_y - read_x).  read_y may be kNoPair.
+// norm_len is the length of the region's longest haplotype: row 0 of the
+// sweep is scaled by 2^120/norm_len, which depends on the region only, so a
+// pair's result does not depend on how the region was cut into chains.
+struct alignas(16) ChainItem {
   uint32_t hap_start;
   uint32_t num_haps;
   uint32_t read_x;
   uint32_t read_y;
   uint32_t out_x;
   uint32_t stride;    // the region's read count
+  uint32_t norm_len;
+  uint32_t pad_;
 };
 
 // Two arbitrary pairs; x has the longer (or equal) haplotype; y.read may be

@@ -485,9 +485,11 @@ struct Forward {
   //   D is set to 0 by the lane after it computes the separator column.
   // So every haplotype sees the reference's column-0 boundary, and the
   // wavefront fills and drains once per chain instead of once per pair.
-  // Row 0 uses one scaling constant for the whole chain, 2^120/Hmax; the DP
-  // is linear in it, so haplotype i's result is rescaled by
-  // (2^120/H_i)/(2^120/Hmax) in FP64 before the acceptance test and log10.
+  // Row 0 uses one scaling constant for the whole chain, 2^120/norm_len
+  // (norm_len: the region's longest haplotype, so no value exceeds the
+  // reference's); the DP is linear in it, so haplotype i's result is
+  // rescaled by (2^120/H_i)/(2^120/norm_len) in FP64 before the acceptance
+  // test and log10.
   __device__ static void run_chain(const BatchView& b, const ClassLaunch& c, uint32_t item,
                                    int lane, uint4* table) {
     ChainMeta* meta = reinterpret_cast<ChainMeta*>(table + Shape::kBytesPerWarp / 16);
@@ -508,25 +510,23 @@ struct Forward {
     const bool bad_hap = (uint32_t)lane < n && (hl == 0 || ((uint32_t)lane + 1 < n &&
                                                             co_next != co + hl + 1));
     const uint32_t Lmax = rx.len > ry.len ? rx.len : ry.len;
-    if (__any_sync(kFullMask, bad_hap) || n == 0 || n > (uint32_t)kChainHaps || rx.len == 0 ||
-        ry.len == 0 || Lmax > (uint32_t)(kWarp * R)) {
+    if (__any_sync(kFullMask, bad_hap || hl > it.norm_len) || n == 0 ||
+        n > (uint32_t)kChainHaps || rx.len == 0 || ry.len == 0 || Lmax > (uint32_t)(kWarp * R)) {
       if (lane == 0) atomicOr(c.error_flags, kErrChain);
       return;
     }
     // end column (exclusive) + 1 of haplotype `lane` in the chain's columns
     uint32_t endc = (uint32_t)lane < n ? hl + 1 : 0;
-    uint32_t hmax = hl;
 #pragma unroll
     for (int d = 1; d < kWarp; d *= 2) {
       const uint32_t v = __shfl_up_sync(kFullMask, endc, d);
       if (lane >= d) endc += v;
-      hmax = max(hmax, __shfl_xor_sync(kFullMask, hmax, d));
     }
     constexpr uint32_t kNever = 0x40000000u;  // beyond every chain's last step
     meta->sep[lane] = ((uint32_t)lane + 1 < n) ? endc - 1 : kNever;
     const uint32_t ncols = __shfl_sync(kFullMask, endc, (int)n - 1) - 1;  // sum H + n - 1
     const uint64_t co0 = __shfl_sync(kFullMask, co, 0);
-    const S init_s = P::init_const() / (S)hmax;
+    const S init_s = P::init_const() / (S)it.norm_len;
     const V init = P::make(init_s, init_s);
     const uint32_t L[2] = {rx.len, ry.len};
     const uint64_t row_off[2] = {rx.row_off, ry.row_off};

@@ -1,0 +1,450 @@
+// service.cpp -- streaming PairHMM service: continuous batching of submitted
+// regions over two device batch slots (see service.h).
+#include "service.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace rodv {
+
+namespace {
+
+constexpr uint64_t kMaxBatchPairs = 1ull << 31;
+
+double ms_between(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+}  // namespace
+
+Service::Service(const rodv_options& opt) : opt_(opt), engine_(opt) {}
+
+Service::~Service() {
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    stop_ = true;
+  }
+  cv_work_.notify_all();
+  cv_space_.notify_all();
+  cv_done_.notify_all();
+  if (thread_.joinable()) thread_.join();  // the worker finishes all submitted work first
+  if (ready_) {
+    for (Slot& s : slots_) {
+      for (cudaEvent_t e : s.ev)
+        if (e) cudaEventDestroy(e);
+      if (s.done) cudaEventDestroy(s.done);
+      if (s.stream) cudaStreamDestroy(s.stream);
+    }
+  }
+}
+
+rodv_status Service::init() {
+  rodv_status st = engine_.init();
+  if (st != RODV_OK) {
+    err_ = engine_.last_error();
+    return st;
+  }
+  ready_ = true;  // streams and events created below are released by the destructor
+  cudaError_t e = cudaSetDevice(engine_.device_);
+  for (Slot& s : slots_) {
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
+    for (cudaEvent_t& ev : s.ev)
+      if (e == cudaSuccess) e = cudaEventCreate(&ev);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+  }
+  size_t free_b = 0, total_b = 0;
+  if (e == cudaSuccess) e = cudaMemGetInfo(&free_b, &total_b);
+  if (e != cudaSuccess) {
+    st = engine_.cuda_fail(e, "service setup");
+    err_ = engine_.last_error();
+    return st;
+  }
+  const uint64_t budget = opt_.device_memory_budget ? opt_.device_memory_budget : free_b / 2;
+  slot_budget_ = budget / 2;
+  max_inflight_ = opt_.max_inflight ? opt_.max_inflight : 4096;
+  thread_ = std::thread([this] { worker(); });
+  return RODV_OK;
+}
+
+// Upper bound of the device bytes one request adds to a batch (the packed
+// layout of engine.cu: codes, row words, descriptors, work items, FP64
+// lists, results, alignment, and the multi-pass boundary scratch when a read
+// needs more than one pass).
+uint64_t Service::estimate_bytes(const rodv_batch& b, uint64_t pairs) const {
+  uint64_t bytes = 4096 + 3 * kNumClasses * 256;
+  uint32_t max_h = 0;
+  bool multi = false;
+  for (uint32_t h = 0; h < b.num_haps; ++h) {
+    bytes += b.hap_lengths[h] + 1;
+    max_h = std::max(max_h, b.hap_lengths[h]);
+  }
+  bytes += 3 * kHapPad + max_h;
+  for (uint32_t r = 0; r < b.num_reads; ++r) {
+    bytes += (uint64_t)((b.read_lengths[r] + 3) & ~3u) * 4;
+    multi = multi || b.read_lengths[r] > (uint32_t)kPassRows;
+  }
+  bytes += (uint64_t)(b.num_haps + b.num_reads) * 16;
+  bytes += pairs * (16 + 12 + 8);
+  // boundary scratch: 24 bytes per column per resident warp of a multi-pass kernel
+  if (multi) bytes += (uint64_t)engine_.num_sms_ * 8 * 4 * (max_h + 40) * 24;
+  return bytes;
+}
+
+rodv_status Service::submit(const rodv_batch& b, uint64_t* ticket) {
+  if (!ticket) return RODV_ERR_INVALID_ARG;
+  uint64_t pairs = 0;
+  std::string msg;
+  const rodv_status st = validate_batch(b, true, &pairs, &msg);
+  auto refuse = [&](rodv_status s, const std::string& m) {
+    std::lock_guard<std::mutex> lk(mu_);
+    err_ = m;
+    return s;
+  };
+  if (st != RODV_OK) return refuse(st, msg);
+  auto r = std::make_shared<Request>();
+  r->pairs = pairs;
+  r->bytes = estimate_bytes(b, pairs);
+  if (r->bytes > slot_budget_ || pairs >= kMaxBatchPairs)
+    return refuse(RODV_ERR_ADMISSION, "request needs ~" + std::to_string(r->bytes) +
+                                          " device bytes; a batch slot holds " +
+                                          std::to_string(slot_budget_));
+  // owned copy, haplotypes and reads rebased to contiguous arrays
+  uint64_t hb = 0, rb = 0;
+  for (uint32_t h = 0; h < b.num_haps; ++h) hb += b.hap_lengths[h];
+  for (uint32_t k = 0; k < b.num_reads; ++k) rb += b.read_lengths[k];
+  r->hap_bases.resize(hb);
+  r->hap_off.resize(b.num_haps);
+  r->hap_len.assign(b.hap_lengths, b.hap_lengths + b.num_haps);
+  for (uint64_t h = 0, o = 0; h < b.num_haps; ++h) {
+    std::memcpy(r->hap_bases.data() + o, b.hap_bases + b.hap_offsets[h], b.hap_lengths[h]);
+    r->hap_off[h] = o;
+    o += b.hap_lengths[h];
+  }
+  r->read_bases.resize(rb);
+  for (auto& q : r->quals) q.resize(rb);
+  r->read_off.resize(b.num_reads);
+  r->read_len.assign(b.read_lengths, b.read_lengths + b.num_reads);
+  const uint8_t* src_q[4] = {b.base_quals, b.ins_quals, b.del_quals, b.gcp_quals};
+  for (uint64_t k = 0, o = 0; k < b.num_reads; ++k) {
+    const uint64_t off = b.read_offsets[k];
+    const uint32_t n = b.read_lengths[k];
+    std::memcpy(r->read_bases.data() + o, b.read_bases + off, n);
+    for (int q = 0; q < 4; ++q) std::memcpy(r->quals[q].data() + o, src_q[q] + off, n);
+    r->read_off[k] = o;
+    o += n;
+  }
+  r->regions.assign(b.regions, b.regions + b.num_regions);
+  for (const rodv_region& rg : r->regions) {
+    uint64_t hs = 0, rs = 0;
+    for (uint32_t h = 0; h < rg.num_haps; ++h) hs += b.hap_lengths[rg.hap_start + h];
+    for (uint32_t k = 0; k < rg.num_reads; ++k) rs += b.read_lengths[rg.read_start + k];
+    r->cells += hs * rs;
+  }
+  {
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_space_.wait(lk, [&] { return stop_ || inflight_ < max_inflight_; });
+    if (stop_) return RODV_ERR_SHUTDOWN;
+    r->ticket = next_ticket_++;
+    r->submitted = Clock::now();
+    if (!st_any_) {
+      st_first_submit_ = r->submitted;
+      st_any_ = true;
+    }
+    ++st_submitted_;
+    ++inflight_;
+    table_[r->ticket] = r;
+    pending_.push_back(r);
+    *ticket = r->ticket;
+  }
+  cv_work_.notify_one();
+  return RODV_OK;
+}
+
+void Service::worker() {
+  cudaSetDevice(engine_.device_);
+  std::deque<int> busy;  // slots with a batch in flight, oldest first
+  for (;;) {
+    int slot = -1;
+    std::vector<std::shared_ptr<Request>> batch;
+    {
+      std::unique_lock<std::mutex> lk(mu_);
+      if (busy.empty()) cv_work_.wait(lk, [&] { return stop_ || !pending_.empty(); });
+      if (busy.empty() && pending_.empty() && stop_) break;
+      if (busy.size() < 2 && !pending_.empty()) {
+        // everything queued, up to one slot's budget, goes into the next batch
+        slot = busy.empty() ? 0 : 1 - busy.front();
+        uint64_t bytes = 0, pairs = 0;
+        while (!pending_.empty()) {
+          const std::shared_ptr<Request>& r = pending_.front();
+          if (!batch.empty() &&
+              (bytes + r->bytes > slot_budget_ || pairs + r->pairs >= kMaxBatchPairs))
+            break;
+          bytes += r->bytes;
+          pairs += r->pairs;
+          batch.push_back(r);
+          pending_.pop_front();
+        }
+      } else if (busy.size() == 1 && pending_.empty()) {
+        // One batch computing and nothing queued: launch a new batch as soon
+        // as something arrives, collect the running one when it is done.
+        if (cudaEventQuery(slots_[busy.front()].done) == cudaErrorNotReady) {
+          cv_work_.wait_for(lk, std::chrono::microseconds(200),
+                            [&] { return stop_ || !pending_.empty(); });
+          continue;
+        }
+      }
+    }
+    if (slot >= 0) {
+      Slot& s = slots_[slot];
+      s.reqs = std::move(batch);
+      s.batch_id = next_batch_++;
+      const Clock::time_point t0 = Clock::now();
+      const rodv_status st = launch(s);
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        st_launch_ms_ += ms_between(t0, Clock::now());
+      }
+      if (st != RODV_OK) {
+        // the slot's stream may still hold part of the batch
+        cudaStreamSynchronize(s.stream);
+        fail_slot(s, st);
+      } else {
+        busy.push_back(slot);
+      }
+      continue;
+    }
+    if (!busy.empty()) {
+      const int i = busy.front();
+      busy.pop_front();
+      complete(slots_[i]);
+    }
+  }
+}
+
+rodv_status Service::launch(Slot& s) {
+  const Clock::time_point t0 = Clock::now();
+  // the combined batch: requests' regions, haplotypes and reads back to back
+  s.regions.clear();
+  s.hap_bases.clear();
+  s.read_bases.clear();
+  for (auto& q : s.quals) q.clear();
+  s.hap_off.clear();
+  s.read_off.clear();
+  s.hap_len.clear();
+  s.read_len.clear();
+  uint64_t est = 0;
+  for (const auto& r : s.reqs) {
+    r->started = t0;
+    est += r->bytes;
+    const uint32_t h0 = (uint32_t)s.hap_len.size(), r0 = (uint32_t)s.read_len.size();
+    const uint64_t hb0 = s.hap_bases.size(), rb0 = s.read_bases.size();
+    for (rodv_region rg : r->regions) {
+      rg.hap_start += h0;
+      rg.read_start += r0;
+      s.regions.push_back(rg);
+    }
+    s.hap_bases.insert(s.hap_bases.end(), r->hap_bases.begin(), r->hap_bases.end());
+    s.read_bases.insert(s.read_bases.end(), r->read_bases.begin(), r->read_bases.end());
+    for (int q = 0; q < 4; ++q)
+      s.quals[q].insert(s.quals[q].end(), r->quals[q].begin(), r->quals[q].end());
+    for (uint64_t o : r->hap_off) s.hap_off.push_back(o + hb0);
+    for (uint64_t o : r->read_off) s.read_off.push_back(o + rb0);
+    s.hap_len.insert(s.hap_len.end(), r->hap_len.begin(), r->hap_len.end());
+    s.read_len.insert(s.read_len.end(), r->read_len.begin(), r->read_len.end());
+  }
+  const rodv_batch b{(uint32_t)s.regions.size(), s.regions.data(), (uint32_t)s.hap_len.size(),
+                     s.hap_bases.data(), s.hap_off.data(), s.hap_len.data(),
+                     (uint32_t)s.read_len.size(), s.read_bases.data(), s.quals[0].data(),
+                     s.quals[1].data(), s.quals[2].data(), s.quals[3].data(),
+                     s.read_off.data(), s.read_len.data()};
+  // Buffers grow with headroom: reallocating device or pinned memory
+  // synchronises the device, which would stall the other slot's batch.
+  if (s.staging.bytes < est) {
+    const cudaError_t e = s.staging.ensure(est + est / 2);
+    if (e != cudaSuccess) return engine_.cuda_fail(e, "service staging");
+  }
+  rodv_status st = engine_.pack(b, s.plan, s.staging, opt_.force_fp64 != 0);
+  if (st != RODV_OK) return st;
+  const PackedPlan& p = s.plan;
+  cudaError_t e = cudaSuccess;
+  if (s.arena.bytes < p.total_bytes) e = s.arena.ensure(p.total_bytes + p.total_bytes / 2);
+  const size_t out_bytes = p.num_pairs * 8 + kCountWords * 4;
+  if (e == cudaSuccess && s.out_host.bytes < out_bytes)
+    e = s.out_host.ensure(out_bytes + out_bytes / 2);
+  if (e != cudaSuccess) return engine_.cuda_fail(e, "service buffers");
+  uint8_t* d = static_cast<uint8_t*>(s.arena.ptr);
+  uint8_t* h = static_cast<uint8_t*>(s.out_host.ptr);
+  e = cudaMemcpyAsync(d, s.staging.ptr, p.upload_bytes, cudaMemcpyHostToDevice, s.stream);
+  if (e != cudaSuccess) return engine_.cuda_fail(e, "service upload");
+  st = engine_.launch_all(p, d, nullptr, s.stream, s.ev, 3);
+  if (st != RODV_OK) return st;
+  e = cudaMemcpyAsync(h, d + p.off_out, p.num_pairs * 8, cudaMemcpyDeviceToHost, s.stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h + p.num_pairs * 8, d + p.off_counts, kCountWords * 4,
+                        cudaMemcpyDeviceToHost, s.stream);
+  if (e == cudaSuccess) e = cudaEventRecord(s.done, s.stream);
+  if (e != cudaSuccess) return engine_.cuda_fail(e, "service download");
+  return RODV_OK;
+}
+
+void Service::complete(Slot& s) {
+  const cudaError_t e = cudaEventSynchronize(s.done);
+  if (e != cudaSuccess) {
+    fail_slot(s, engine_.cuda_fail(e, "service batch"));
+    return;
+  }
+  const Clock::time_point t0 = Clock::now();
+  const PackedPlan& p = s.plan;
+  const uint8_t* h = static_cast<const uint8_t*>(s.out_host.ptr);
+  const uint32_t* counts = reinterpret_cast<const uint32_t*>(h + p.num_pairs * 8);
+  if (counts[kCtrError] != 0) {
+    fail_slot(s, engine_.fail(RODV_ERR_DEVICE_CHECK, "kernel reported error flags " +
+                                                         std::to_string(counts[kCtrError])));
+    return;
+  }
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, s.ev[0], s.ev[2]);
+  uint64_t fp64 = 0;
+  for (int c = 0; c < kNumClasses; ++c) fp64 += p.fp64 ? p.pairs[c] : counts[kCtrRescue + c];
+  const double* res = reinterpret_cast<const double*>(h);
+  uint64_t off = 0;
+  for (const auto& r : s.reqs) {
+    r->out.assign(res + off, res + off + r->pairs);
+    off += r->pairs;
+    r->fp64_pairs = fp64;
+    r->batch_id = s.batch_id;
+    r->batch_regions = (uint32_t)s.regions.size();
+  }
+  const Clock::time_point now = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    for (const auto& r : s.reqs) {
+      r->finished = now;
+      r->status = RODV_OK;
+      r->done = true;
+      latencies_.push_back(ms_between(r->submitted, now));
+      ++st_completed_;
+      st_pairs_ += r->pairs;
+      st_cells_ += r->cells;
+      st_regions_ += r->regions.size();
+      --inflight_;
+    }
+    st_fp64_ += fp64;
+    st_device_ms_ += ms;
+    st_finish_ms_ += ms_between(t0, now);
+    ++st_batches_;
+    st_last_done_ = now;
+  }
+  if (opt_.verbose)
+    fprintf(stderr, "rodv service: batch %llu: %zu requests, %zu regions, %llu pairs, %.3f ms\n",
+            (unsigned long long)s.batch_id, s.reqs.size(), s.regions.size(),
+            (unsigned long long)p.num_pairs, ms);
+  s.reqs.clear();
+  cv_done_.notify_all();
+  cv_space_.notify_all();
+}
+
+void Service::fail_slot(Slot& s, rodv_status st) {
+  const Clock::time_point now = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    err_ = engine_.last_error();
+    for (const auto& r : s.reqs) {
+      r->finished = now;
+      r->status = st;
+      r->done = true;
+      ++st_failed_;
+      --inflight_;
+    }
+  }
+  s.reqs.clear();
+  cv_done_.notify_all();
+  cv_space_.notify_all();
+}
+
+rodv_status Service::result(uint64_t ticket, int32_t wait_ms, double* out,
+                            rodv_request_stats* st) {
+  std::shared_ptr<Request> r;
+  {
+    std::unique_lock<std::mutex> lk(mu_);
+    auto it = table_.find(ticket);
+    if (it == table_.end()) return RODV_ERR_NOT_FOUND;
+    r = it->second;
+    if (!r->done) {
+      if (wait_ms == 0) return RODV_ERR_NOT_READY;
+      auto ready = [&] { return r->done; };
+      if (wait_ms < 0)
+        cv_done_.wait(lk, ready);
+      else if (!cv_done_.wait_for(lk, std::chrono::milliseconds(wait_ms), ready))
+        return RODV_ERR_NOT_READY;
+    }
+    table_.erase(ticket);
+  }
+  if (r->status != RODV_OK) return r->status;
+  if (out) std::memcpy(out, r->out.data(), r->pairs * sizeof(double));
+  if (st) {
+    *st = rodv_request_stats{};
+    st->pairs = r->pairs;
+    st->cells = r->cells;
+    st->fp64_pairs = r->fp64_pairs;
+    st->batch_id = r->batch_id;
+    st->batch_regions = r->batch_regions;
+    st->queue_ms = ms_between(r->submitted, r->started);
+    st->latency_ms = ms_between(r->submitted, r->finished);
+  }
+  return RODV_OK;
+}
+
+rodv_status Service::stats(rodv_service_stats* out) {
+  if (!out) return RODV_ERR_INVALID_ARG;
+  std::vector<double> lat;
+  *out = rodv_service_stats{};
+  {
+    std::lock_guard<std::mutex> lk(mu_);
+    lat = latencies_;
+    out->submitted = st_submitted_;
+    out->completed = st_completed_;
+    out->failed = st_failed_;
+    out->batches = st_batches_;
+    out->regions = st_regions_;
+    out->pairs = st_pairs_;
+    out->cells = st_cells_;
+    out->fp64_pairs = st_fp64_;
+    out->device_ms = st_device_ms_;
+    out->wall_ms = (st_any_ && st_completed_) ? ms_between(st_first_submit_, st_last_done_) : 0.0;
+    out->mean_batch_regions = st_batches_ ? (double)st_regions_ / st_batches_ : 0.0;
+    out->host_launch_ms = st_launch_ms_;
+    out->host_finish_ms = st_finish_ms_;
+  }
+  if (!lat.empty()) {
+    std::sort(lat.begin(), lat.end());
+    auto pct = [&](double q) {  // nearest rank
+      const size_t k = (size_t)std::ceil(q * (double)lat.size());
+      return lat[std::min(lat.size(), std::max<size_t>(k, 1)) - 1];
+    };
+    out->latency_p50_ms = pct(0.50);
+    out->latency_p99_ms = pct(0.99);
+    out->latency_max_ms = lat.back();
+    double sum = 0;
+    for (double v : lat) sum += v;
+    out->latency_mean_ms = sum / (double)lat.size();
+  }
+  return RODV_OK;
+}
+
+std::string Service::last_error() {
+  std::lock_guard<std::mutex> lk(mu_);
+  return err_;
+}
+
+void Service::reset_stats() {
+  std::lock_guard<std::mutex> lk(mu_);
+  latencies_.clear();
+  st_submitted_ = st_completed_ = st_failed_ = st_batches_ = 0;
+  st_pairs_ = st_cells_ = st_fp64_ = st_regions_ = 0;
+  st_device_ms_ = st_launch_ms_ = st_finish_ms_ = 0;
+  st_any_ = false;
+}
+
+}  // namespace rodv

@@ -98,3 +98,21 @@ def test_python_engine_raises_without_device():
     with pytest.raises(RodvError) as ei:
         Engine(0)
     assert ei.value.status == 4
+
+
+def test_service_create_without_device_fails_cleanly():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    assert lib.rodv_service_create(None, ctypes.byref(h)) == 4  # RODV_ERR_NO_DEVICE
+    assert not h.value
+    # calls on a null service are argument errors, never crashes
+    t = ctypes.c_uint64()
+    assert lib.rodv_submit_region(None, None, ctypes.byref(t)) == 1
+    assert lib.rodv_poll(None, 1, None, None) == 1
+    assert lib.rodv_service_last_error(None) == b""
