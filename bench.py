@@ -392,7 +392,7 @@ def streaming_c5(args):
     pool = [pool_batch.subset([g]) for g in range(pool_batch.num_regions)]
     holders = [_CBatchHolder(b) for b in pool]
     cells = [b.cells() for b in pool]
-    sv = Service(0)
+    sv = Service(0, verbose=args.stream_verbose)
     lib, h = sv.lib, sv.h
 
     def run(n_req, rate):
@@ -514,6 +514,8 @@ def main():
                     help="streaming (C5): regions in the cycled pool")
     ap.add_argument("--stream-requests", type=int, default=1200,
                     help="streaming (C5): requests of the saturation run (0: skip C5)")
+    ap.add_argument("--stream-verbose", type=int, default=0,
+                    help="streaming (C5): service verbosity (2: host time sections)")
     ap.add_argument("--stream-seconds", type=float, default=3.0,
                     help="streaming (C5): seconds of arrivals per Poisson rate")
     args = ap.parse_args()

@@ -73,6 +73,26 @@ void parallel_for(size_t n, size_t grain, F&& f) {
   for (auto& th : pool) th.join();
 }
 
+// Section timer of the packer, printed at verbose level 2.
+struct PackTimer {
+  bool on;
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  std::string line;
+  explicit PackTimer(bool enabled) : on(enabled) {}
+  void mark(const char* what) {
+    if (!on) return;
+    const auto now = std::chrono::steady_clock::now();
+    char buf[64];
+    snprintf(buf, sizeof(buf), " %s %.2f", what,
+             std::chrono::duration<double, std::milli>(now - t).count());
+    line += buf;
+    t = now;
+  }
+  ~PackTimer() {
+    if (on) fprintf(stderr, "rodv: pack ms:%s\n", line.c_str());
+  }
+};
+
 double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -276,6 +296,7 @@ rodv_status validate_batch(const rodv_batch& b, bool check_bases, uint64_t* num_
 }
 
 rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64) {
+  PackTimer timer(opt_.verbose >= 2);
   plan = PackedPlan{};
   plan.fp64 = fp64;
   uint64_t pairs = 0;
@@ -320,6 +341,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   }
   plan.read_rows = rows;
 
+  timer.mark("validate+offsets");
   // ---- read flags (uniform gaps) and class of every read ----
   std::vector<uint8_t>& read_class = plan.read_class;
   read_class.resize(b.num_reads);
@@ -339,6 +361,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
     }
   });
 
+  timer.mark("classes");
   // ---- per region and class: reads, chain items, same items, leftovers ----
   // Single-pass reads of a region are sorted by (uniform gaps, length) and
   // paired neighbour by neighbour; a pair's class is that of its longer read
@@ -475,6 +498,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
         plan.multi_max_hap = std::max(plan.multi_max_hap, b.hap_lengths[rg.hap_start + h]);
   }
 
+  timer.mark("pairing");
   // ---- arena layout ----
   size_t o = 0;
   plan.off_hap_codes = o; o = align_up(o + hb);
@@ -524,6 +548,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   if (e != cudaSuccess) return cuda_fail(e, "pinned staging allocation");
   uint8_t* s = static_cast<uint8_t*>(staging.ptr);
 
+  timer.mark("layout+staging");
   // ---- haplotype codes ----
   std::atomic<int> bad_base{-1};
   uint8_t* codes = s + plan.off_hap_codes;
@@ -546,6 +571,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   });
   std::memset(codes, 0, kHapPad);
   std::memset(codes + tail_begin, 0, hb - tail_begin);
+  timer.mark("haps");
   // ---- read rows ----
   uint32_t* rw = reinterpret_cast<uint32_t*>(s + plan.off_read_rows);
   ReadDesc* rdesc = reinterpret_cast<ReadDesc*>(s + plan.off_reads);
@@ -576,6 +602,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
     uint32_t* preset = reinterpret_cast<uint32_t*>(s + plan.off_preset);
     for (int c = 0; c < kNumClasses; ++c) preset[c] = plan.pairs[c];
   }
+  timer.mark("rows");
   // ---- work: chain items, same-haplotype items, leftovers, forced-FP64 lists ----
   std::vector<uint64_t> region_out(G);
   for (uint32_t g = 0, acc = 0; g < G; ++g) {
@@ -654,6 +681,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
         return fail(RODV_ERR_INTERNAL, "leftover pairing count mismatch");
     }
   }
+  timer.mark("work");
   // cells
   uint64_t cells = 0;
   for (uint32_t g = 0; g < G; ++g) {

@@ -11,6 +11,19 @@ namespace rodv {
 namespace {
 
 constexpr uint64_t kMaxBatchPairs = 1ull << 31;
+// A batch holds up to this many estimated device bytes (~600 regions of
+// 1-32 haplotypes x 1-300 reads; tens of ms of GPU work), unless one request
+// alone is larger.  Each slot's buffers are reserved for it at creation, so
+// steady-state batches never reallocate (a pinned or device reallocation
+// synchronises the device and costs far more than packing a batch).
+constexpr uint64_t kBatchBytes = 128ull << 20;
+
+// Grows a buffer to at least n bytes, at least doubling it.
+template <class Mem>
+cudaError_t grow(Mem& m, size_t n) {
+  if (m.ptr && m.bytes >= n) return cudaSuccess;
+  return m.ensure(std::max(n + n / 4, 2 * m.bytes));
+}
 
 double ms_between(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
@@ -62,7 +75,19 @@ rodv_status Service::init() {
   }
   const uint64_t budget = opt_.device_memory_budget ? opt_.device_memory_budget : free_b / 2;
   slot_budget_ = budget / 2;
+  batch_bytes_ = std::min<uint64_t>(slot_budget_, kBatchBytes);
   max_inflight_ = opt_.max_inflight ? opt_.max_inflight : 4096;
+  for (Slot& s : slots_) {
+    // staging holds at most the estimate; results are 8 of its ~36 bytes per pair
+    if (e == cudaSuccess) e = s.staging.ensure(batch_bytes_);
+    if (e == cudaSuccess) e = s.arena.ensure(batch_bytes_);
+    if (e == cudaSuccess) e = s.out_host.ensure(batch_bytes_ / 4 + kCountWords * 4);
+  }
+  if (e != cudaSuccess) {
+    st = engine_.cuda_fail(e, "service buffers");
+    err_ = engine_.last_error();
+    return st;
+  }
   thread_ = std::thread([this] { worker(); });
   return RODV_OK;
 }
@@ -178,7 +203,7 @@ void Service::worker() {
         while (!pending_.empty()) {
           const std::shared_ptr<Request>& r = pending_.front();
           if (!batch.empty() &&
-              (bytes + r->bytes > slot_budget_ || pairs + r->pairs >= kMaxBatchPairs))
+              (bytes + r->bytes > batch_bytes_ || pairs + r->pairs >= kMaxBatchPairs))
             break;
           bytes += r->bytes;
           pairs += r->pairs;
@@ -253,6 +278,7 @@ rodv_status Service::launch(Slot& s) {
     s.hap_len.insert(s.hap_len.end(), r->hap_len.begin(), r->hap_len.end());
     s.read_len.insert(s.read_len.end(), r->read_len.begin(), r->read_len.end());
   }
+  const Clock::time_point t_comb = Clock::now();
   const rodv_batch b{(uint32_t)s.regions.size(), s.regions.data(), (uint32_t)s.hap_len.size(),
                      s.hap_bases.data(), s.hap_off.data(), s.hap_len.data(),
                      (uint32_t)s.read_len.size(), s.read_bases.data(), s.quals[0].data(),
@@ -260,18 +286,17 @@ rodv_status Service::launch(Slot& s) {
                      s.read_off.data(), s.read_len.data()};
   // Buffers grow with headroom: reallocating device or pinned memory
   // synchronises the device, which would stall the other slot's batch.
-  if (s.staging.bytes < est) {
-    const cudaError_t e = s.staging.ensure(est + est / 2);
+  {
+    const cudaError_t e = grow(s.staging, est);
     if (e != cudaSuccess) return engine_.cuda_fail(e, "service staging");
   }
+  const Clock::time_point t_stage = Clock::now();
   rodv_status st = engine_.pack(b, s.plan, s.staging, opt_.force_fp64 != 0);
   if (st != RODV_OK) return st;
+  const Clock::time_point t_pack = Clock::now();
   const PackedPlan& p = s.plan;
-  cudaError_t e = cudaSuccess;
-  if (s.arena.bytes < p.total_bytes) e = s.arena.ensure(p.total_bytes + p.total_bytes / 2);
-  const size_t out_bytes = p.num_pairs * 8 + kCountWords * 4;
-  if (e == cudaSuccess && s.out_host.bytes < out_bytes)
-    e = s.out_host.ensure(out_bytes + out_bytes / 2);
+  cudaError_t e = grow(s.arena, p.total_bytes);
+  if (e == cudaSuccess) e = grow(s.out_host, p.num_pairs * 8 + kCountWords * 4);
   if (e != cudaSuccess) return engine_.cuda_fail(e, "service buffers");
   uint8_t* d = static_cast<uint8_t*>(s.arena.ptr);
   uint8_t* h = static_cast<uint8_t*>(s.out_host.ptr);
@@ -285,6 +310,12 @@ rodv_status Service::launch(Slot& s) {
                         cudaMemcpyDeviceToHost, s.stream);
   if (e == cudaSuccess) e = cudaEventRecord(s.done, s.stream);
   if (e != cudaSuccess) return engine_.cuda_fail(e, "service download");
+  if (opt_.verbose >= 2)
+    fprintf(stderr,
+            "rodv service: batch %llu launch ms: combine %.2f staging %.2f pack %.2f "
+            "enqueue %.2f (%zu regions)\n",
+            (unsigned long long)s.batch_id, ms_between(t0, t_comb), ms_between(t_comb, t_stage),
+            ms_between(t_stage, t_pack), ms_between(t_pack, Clock::now()), s.regions.size());
   return RODV_OK;
 }
 

@@ -7,7 +7,9 @@
 // host packs and uploads batch k+1 while the kernels of batch k run.
 // Admission: a request larger than a slot's share of the device-memory
 // budget is refused (RODV_ERR_ADMISSION); submit blocks while max_inflight
-// requests are queued or running.
+// requests are queued or running.  A batch takes queued requests up to a
+// fixed size (or one larger request alone) so that its buffers, reserved at
+// creation, are reused without reallocation.
 #pragma once
 #include <chrono>
 #include <condition_variable>
@@ -78,7 +80,8 @@ class Service {
   rodv_options opt_;
   Engine engine_;
   Slot slots_[2];
-  uint64_t slot_budget_ = 0;
+  uint64_t slot_budget_ = 0;   // largest request (device bytes) a slot admits
+  uint64_t batch_bytes_ = 0;   // batches are formed up to this size
   uint32_t max_inflight_ = 0;
 
   std::mutex mu_;
