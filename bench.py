@@ -276,9 +276,10 @@ def run_engine(args, world, rank, local):
         achieved = FLOPS_PER_CELL * cells / fp32_avg_s / 1e12
         peak = peaks["fp32_gflops"] / 1e3
         plain = plain_form(eng, args) if args.plain_pairs > 0 else None
+        configs = config_lines(eng, args, value) if not args.no_configs else None
         cpu = None
         if not args.no_cpu_baseline:
-            cpu = cpu_baseline(args)
+            cpu = cpu_baseline(args, eng)
         stream = streaming_c5(args) if args.stream_requests > 0 else None
         line = {
             "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world,
@@ -319,6 +320,8 @@ def run_engine(args, world, rank, local):
             line["plain_form"] = plain
         if cpu:
             line["cpu_baseline"] = cpu
+        if configs:
+            line["configs"] = configs
         if stream:
             line["streaming"] = stream
         print(json.dumps(line), flush=True)
@@ -476,7 +479,77 @@ def streaming_c5(args):
             "saturation": sat, "saturation_regions_per_s": sat_rate, "poisson": runs}
 
 
-def cpu_baseline(args):
+# The configurations of the benchmark, by the workload generator that makes
+# them: (name, workload, scale for the GPU throughput run, description).
+CONFIGS = [
+    ("C1", "plain", 1.0, "1 region: 8 haplotypes of 250-400 bases x 64 reads of 150 bases"),
+    ("C2", "uneven", 1.0, "10,000 regions: 2-16 haplotypes of 100-600 bases x 20-200 reads "
+                          "of 50-250 bases"),
+    ("C3", "long", 1.0, "2,000 pairs: reads of 1,000-2,000 bases x haplotypes of "
+                        "2,000-5,000 bases"),
+    ("C4", "underflow", 1.0, "200,000 pairs: 250-base reads (base quals 2-8) x independent "
+                             "400-base haplotypes; every pair rescued in FP64"),
+    ("C5", "stream", 0.3, "300 regions of the streaming shape: 1-32 haplotypes of 100-800 "
+                          "bases x 1-300 reads of 50-250 bases (resident, as one batch)"),
+]
+
+
+def config_lines(eng, args, c2_value):
+    """GPU throughput of every configuration (resident batch, CUDA events) and
+    its FP64 rescue rate; C2 is the headline line itself."""
+    from rodv_b200 import workloads
+    lines = []
+    for name, wl, scale, desc in CONFIGS:
+        if name == "C2":
+            lines.append({"config": name, "what": desc, "gcups": c2_value, "see": "value"})
+            continue
+        b = workloads.make_workload(wl, seed=workloads.SEEDS[wl], scale=scale)
+        db = eng.upload(b)
+        db.run()
+        sts = [db.run() for _ in range(3)]
+        db.free()
+        dev = min(x["device_ms"] for x in sts)
+        lines.append({"config": name, "what": desc, "regions": b.num_regions,
+                      "pairs": b.num_pairs, "cells": b.cells(), "device_ms": dev,
+                      "gcups": b.cells() / (dev / 1e3) / 1e9,
+                      "fp64_rescue_rate": sts[-1]["fp64_pairs"] / b.num_pairs})
+    return lines
+
+
+# Accuracy samples per configuration: (name, workload, scale of the sample the
+# FP64 oracle computes, scale of the sample the reference computes).
+ACCURACY_SAMPLES = [("C1", "plain", 1.0, 1.0), ("C2", "uneven", 0.001, 0.02),
+                    ("C3", "long", 0.01, 0.1), ("C4", "underflow", 0.005, 0.1),
+                    ("C5", "stream", 0.004, 0.05)]
+
+
+def accuracy_per_config(eng):
+    """|delta log10| of the engine's results against the FP64 oracle (FP64 DP
+    with per-row rescaling, so no pair underflows: the exact value up to FP64
+    rounding) and against the reference's schedule_pairhmm, on seeded samples
+    of every configuration."""
+    import oracle
+    from rodv_b200 import workloads
+    out = []
+    for name, wl, s_oracle, s_ref in ACCURACY_SAMPLES:
+        row = {"config": name}
+        for key, scale in (("vs_fp64_oracle", s_oracle), ("vs_reference", s_ref)):
+            b = workloads.make_workload(wl, seed=workloads.SEEDS[wl] + 99, scale=scale)
+            got = eng.batch(b)
+            ref = (oracle.batch_log10(b, oracle.SCALED) if key == "vs_fp64_oracle"
+                   else oracle.ref_schedule(b))
+            fin = np.isfinite(ref) & np.isfinite(got)
+            d = np.abs(got[fin] - ref[fin])
+            row[key] = {"pairs": int(b.num_pairs), "cells": b.cells(),
+                        "max": float(d.max()) if d.size else None,
+                        "mean": float(d.mean()) if d.size else None,
+                        "non_finite_mismatches": int(np.sum(np.isfinite(ref) !=
+                                                            np.isfinite(got)))}
+        out.append(row)
+    return out
+
+
+def cpu_baseline(args, eng=None):
     import oracle
     if not oracle.ref_available():
         return {"value": None, "unit": "GCUPS", "cores": 0, "kind": "reference",
@@ -484,11 +557,14 @@ def cpu_baseline(args):
     threads = os.cpu_count() or 1
     batch = sized_sample(args.workload, 7000, args.cpu_seconds, threads)
     rate, dt = reference_rate(batch, threads)
-    return {"value": rate, "unit": "GCUPS", "cores": threads, "kind": "reference",
-            "sample": f"{batch.num_regions} regions / {batch.num_pairs} pairs / "
-                      f"{batch.cells():.3e} cells of the {args.workload} workload, "
-                      f"{dt:.1f} s on {threads} threads",
-            "cpu": cpu_model()}
+    res = {"value": rate, "unit": "GCUPS", "cores": threads, "kind": "reference",
+           "sample": f"{batch.num_regions} regions / {batch.num_pairs} pairs / "
+                     f"{batch.cells():.3e} cells of the {args.workload} workload, "
+                     f"{dt:.1f} s on {threads} threads",
+           "cpu": cpu_model()}
+    if eng is not None:
+        res["accuracy_per_config"] = accuracy_per_config(eng)
+    return res
 
 
 def main():
@@ -505,6 +581,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--plain-pairs", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the per-configuration throughput lines (C1, C3-C5)")
     ap.add_argument("--tune", action="store_true", help="profile mode: autotune first")
     ap.add_argument("--ref-seconds", type=float, default=6.0,
                     help="reference arm: wall seconds of CPU work per step")

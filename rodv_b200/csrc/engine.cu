@@ -163,6 +163,13 @@ Engine::~Engine() {
     cudaStreamSynchronize(stream_);
     for (auto& e : ev_) cudaEventDestroy(e);
     cudaStreamDestroy(stream_);
+    for (HostLane& l : lanes_) {
+      if (l.stream) cudaStreamSynchronize(l.stream);
+      for (cudaEvent_t e : l.ev)
+        if (e) cudaEventDestroy(e);
+      if (l.done) cudaEventDestroy(l.done);
+      if (l.stream) cudaStreamDestroy(l.stream);
+    }
   }
 }
 
@@ -201,6 +208,12 @@ rodv_status Engine::init() {
   device_name_ = prop.name;
   RODV_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   for (auto& e : ev_) RODV_CUDA(cudaEventCreate(&e));
+  ready_ = true;  // the destructor releases what was created
+  for (HostLane& l : lanes_) {
+    RODV_CUDA(cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking));
+    for (auto& e : l.ev) RODV_CUDA(cudaEventCreate(&e));
+    RODV_CUDA(cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming));
+  }
   const HostPriorTables& t = host_prior_tables();
   const size_t bytes = 128 * 4 + kMmTableSize * 4 + 128 * 8 + kMmTableSize * 8 + 4 * kAlign;
   RODV_CUDA(tables_.ensure(bytes));
@@ -422,8 +435,9 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   });
   // Haplotypes per chain item, per class: the longest chains (up to
   // kChainHaps) that still leave every resident warp of the class's launch
-  // several items; a small batch gets short chains (down to one haplotype).
-  const uint64_t target_items = (uint64_t)num_sms_ * 16 * 4;
+  // (16 per SM at most) two items; a small batch gets short chains (down to
+  // one haplotype).
+  const uint64_t target_items = (uint64_t)num_sms_ * 16 * 2;
   for (int c = 0; c < kSinglePassClasses; ++c) {
     plan.chain_haps[c] = 1;
     for (uint32_t cap = kChainHaps; cap >= 1; cap /= 2) {
@@ -784,12 +798,184 @@ static void fill_stats(rodv_stats* st, const PackedPlan& plan, const uint32_t* c
   st->fp64_pairs = n;
 }
 
+// Host buffers in and out.  A large batch is cut into region ranges that go
+// through two lanes: while one range computes, the host packs the next into
+// the other lane's staging buffer and its upload runs on the copy engine, so
+// packing and transfers hide behind the kernels.  Range sizes start small
+// (the first range's packing and upload are not hidden) and double up to
+// kChunkCells cells.  Results do not depend on the cut (a pair's arithmetic
+// depends on its own region only).
+constexpr double kChunkCells = 6e10;
+constexpr double kFirstChunkCells = 4e9;
+constexpr double kMinChunkedCells = 2e10;
+
 rodv_status Engine::run_host(const rodv_batch& b, double* out, rodv_stats* st, bool force_fp64) {
   if (!out) return fail(RODV_ERR_INVALID_ARG, "null output");
-  const auto t0 = std::chrono::steady_clock::now();
   RODV_CUDA(cudaSetDevice(device_));
+  const bool fp64 = force_fp64 || opt_.force_fp64 != 0;
+  {
+    std::string msg;
+    const rodv_status vs = validate_batch(b, false, nullptr, &msg);
+    if (vs != RODV_OK) return fail(vs, msg);
+  }
+  const uint32_t G = b.num_regions;
+  std::vector<double> cum(G + 1, 0.0);
+  for (uint32_t g = 0; g < G; ++g) {
+    const rodv_region& rg = b.regions[g];
+    double hs = 0, rs = 0;
+    for (uint32_t h = 0; h < rg.num_haps; ++h) hs += b.hap_lengths[rg.hap_start + h];
+    for (uint32_t r = 0; r < rg.num_reads; ++r) rs += b.read_lengths[rg.read_start + r];
+    cum[g + 1] = cum[g] + hs * rs;
+  }
+  if (cum[G] < kMinChunkedCells || G < 4) return run_host_single(b, out, st, fp64);
+  std::vector<uint32_t> bounds{0};
+  double target = std::min(kChunkCells, std::max(kFirstChunkCells, cum[G] / 32));
+  for (uint32_t g = 1; g < G; ++g) {
+    if (cum[g] - cum[bounds.back()] >= target) {
+      bounds.push_back(g);
+      target = std::min(kChunkCells, 2 * target);
+    }
+  }
+  bounds.push_back(G);
+  if (bounds.size() < 3) return run_host_single(b, out, st, fp64);
+  return run_host_chunked(b, out, st, fp64, bounds);
+}
+
+rodv_status Engine::finish_lane(HostLane& l, double* out, rodv_stats* st) {
+  l.busy = false;
+  RODV_CUDA(cudaEventSynchronize(l.done));
+  const PackedPlan& p = l.plan;
+  const uint8_t* h = static_cast<const uint8_t*>(l.out.ptr);
+  const uint32_t* counts = reinterpret_cast<const uint32_t*>(h + p.num_pairs * 8);
+  if (counts[kCtrError] != 0)
+    return fail(RODV_ERR_DEVICE_CHECK,
+                "kernel reported error flags " + std::to_string(counts[kCtrError]));
+  std::memcpy(out + l.out_off, h, p.num_pairs * 8);
+  if (st) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, l.ev[0], l.ev[2]);
+    st->device_ms += ms;
+    cudaEventElapsedTime(&ms, l.ev[0], l.ev[1]);
+    st->fp32_ms += ms;
+    cudaEventElapsedTime(&ms, l.ev[3], l.ev[0]);
+    st->h2d_ms += ms;
+    st->h2d_bytes += p.upload_bytes;
+    st->d2h_bytes += p.num_pairs * 8 + kCountWords * 4;
+    st->pairs += p.num_pairs;
+    st->cells += p.cells;
+    for (int c = 0; c < kNumClasses; ++c)
+      st->fp64_pairs += p.fp64 ? p.pairs[c] : counts[kCtrRescue + c];
+  }
+  return RODV_OK;
+}
+
+rodv_status Engine::run_host_chunked(const rodv_batch& b, double* out, rodv_stats* st,
+                                     bool fp64, const std::vector<uint32_t>& bounds) {
+  const auto t0 = std::chrono::steady_clock::now();
+  rodv_stats acc{};
+  const size_t nchunks = bounds.size() - 1;
+  rodv_status result = RODV_OK;
+  uint64_t out_off = 0;
+  for (size_t k = 0; k < nchunks && result == RODV_OK; ++k) {
+    HostLane& l = lanes_[k & 1];
+    if (l.busy) {
+      result = finish_lane(l, out, &acc);
+      if (result != RODV_OK) break;
+    }
+    // the range's regions over the batch's arrays, rebased to the range's
+    // first haplotype and read
+    const uint32_t g0 = bounds[k], g1 = bounds[k + 1];
+    uint32_t h0 = UINT32_MAX, h1 = 0, r0 = UINT32_MAX, r1 = 0;
+    uint64_t pairs = 0;
+    for (uint32_t g = g0; g < g1; ++g) {
+      const rodv_region& rg = b.regions[g];
+      h0 = std::min(h0, rg.hap_start);
+      h1 = std::max(h1, rg.hap_start + rg.num_haps);
+      r0 = std::min(r0, rg.read_start);
+      r1 = std::max(r1, rg.read_start + rg.num_reads);
+      pairs += (uint64_t)rg.num_haps * rg.num_reads;
+    }
+    l.regs.assign(b.regions + g0, b.regions + g1);
+    for (rodv_region& rg : l.regs) {
+      rg.hap_start -= h0;
+      rg.read_start -= r0;
+    }
+    const rodv_batch v{g1 - g0, l.regs.data(), h1 - h0, b.hap_bases, b.hap_offsets + h0,
+                       b.hap_lengths + h0, r1 - r0, b.read_bases, b.base_quals, b.ins_quals,
+                       b.del_quals, b.gcp_quals, b.read_offsets + r0, b.read_lengths + r0};
+    {
+      // Upper bound of the upload (codes, row words, descriptors, items, lists),
+      // reserved with headroom: regrowing pinned memory synchronises the device.
+      uint64_t est = 1u << 20;
+      for (uint32_t x = h0; x < h1; ++x) est += b.hap_lengths[x] + 1 + 16;
+      for (uint32_t x = r0; x < r1; ++x) est += ((b.read_lengths[x] + 3) & ~3u) * 4 + 16;
+      est += pairs * (fp64 ? 12 : 16);
+      if (l.staging.bytes < est) {
+        const cudaError_t e = l.staging.ensure(est + est / 4);
+        if (e != cudaSuccess) {
+          result = cuda_fail(e, "chunk staging");
+          break;
+        }
+      }
+    }
+    result = pack(v, l.plan, l.staging, fp64);
+    if (result != RODV_OK) break;
+    const PackedPlan& p = l.plan;
+    cudaError_t e = cudaSuccess;
+    if (l.arena.bytes < p.total_bytes) e = l.arena.ensure(p.total_bytes + p.total_bytes / 4);
+    const size_t ob = p.num_pairs * 8 + kCountWords * 4;
+    if (e == cudaSuccess && l.out.bytes < ob) e = l.out.ensure(ob + ob / 4);
+    uint8_t* d = static_cast<uint8_t*>(l.arena.ptr);
+    uint8_t* h = static_cast<uint8_t*>(l.out.ptr);
+    if (e == cudaSuccess) e = cudaEventRecord(l.ev[3], l.stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d, l.staging.ptr, p.upload_bytes, cudaMemcpyHostToDevice, l.stream);
+    if (e != cudaSuccess) {
+      result = cuda_fail(e, "chunk upload");
+      break;
+    }
+    result = launch_all(p, d, &acc, l.stream, l.ev, 3);
+    if (result != RODV_OK) break;
+    e = cudaMemcpyAsync(h, d + p.off_out, p.num_pairs * 8, cudaMemcpyDeviceToHost, l.stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h + p.num_pairs * 8, d + p.off_counts, kCountWords * 4,
+                          cudaMemcpyDeviceToHost, l.stream);
+    if (e == cudaSuccess) e = cudaEventRecord(l.done, l.stream);
+    if (e != cudaSuccess) {
+      result = cuda_fail(e, "chunk download");
+      break;
+    }
+    l.out_off = out_off;
+    l.busy = true;
+    out_off += pairs;
+  }
+  // collect what is still in flight, oldest first (on error too: no lane may
+  // be left with work that writes into buffers reused by the next call)
+  for (size_t k = nchunks; k < nchunks + 2; ++k) {
+    HostLane& l = lanes_[k & 1];
+    if (!l.busy) continue;
+    if (result == RODV_OK) {
+      result = finish_lane(l, out, &acc);
+    } else {
+      cudaStreamSynchronize(l.stream);
+      l.busy = false;
+    }
+  }
+  if (result != RODV_OK) return result;
+  if (st) {
+    const uint32_t launches = st->kernel_launches + acc.kernel_launches;
+    *st = acc;
+    st->kernel_launches = launches;
+    st->total_ms = ms_since(t0);
+  }
+  return RODV_OK;
+}
+
+rodv_status Engine::run_host_single(const rodv_batch& b, double* out, rodv_stats* st,
+                                    bool fp64) {
+  const auto t0 = std::chrono::steady_clock::now();
   PackedPlan plan;
-  rodv_status s = pack(b, plan, staging_, force_fp64 || opt_.force_fp64 != 0);
+  rodv_status s = pack(b, plan, staging_, fp64);
   if (s != RODV_OK) return s;
   RODV_CUDA(arena_.ensure(plan.total_bytes));
   RODV_CUDA(out_staging_.ensure(plan.num_pairs * 8 + kCountWords * 4));

@@ -111,6 +111,20 @@ class Engine {
   rodv_status autotune(const char* cache_path, int force, int32_t* variants_out);
 
   std::mutex& mutex() { return mu_; }
+  // One stage of the chunked host-buffer path: a region range packed,
+  // uploaded, computed and downloaded on its own stream while the host packs
+  // the next range into the other lane.
+  struct HostLane {
+    PackedPlan plan;
+    PinnedMem staging, out;
+    DeviceMem arena;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {};        // FP32 start, FP32 end, FP64 end, upload start
+    cudaEvent_t done = nullptr;    // after the result download
+    std::vector<rodv_region> regs;
+    uint64_t out_off = 0;
+    bool busy = false;
+  };
   const char* last_error() const { return last_error_.c_str(); }
   rodv_status fail(rodv_status s, const std::string& msg);
   rodv_status cuda_fail(cudaError_t e, const char* where);
@@ -125,6 +139,10 @@ class Engine {
   rodv_status launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, int cls, bool same,
                                 int variant, int blocks_cap, cudaStream_t stream);
   rodv_status check_errors(const PackedPlan& plan, uint8_t* dbase);
+  rodv_status run_host_single(const rodv_batch& b, double* out, rodv_stats* st, bool fp64);
+  rodv_status run_host_chunked(const rodv_batch& b, double* out, rodv_stats* st, bool fp64,
+                               const std::vector<uint32_t>& bounds);
+  rodv_status finish_lane(HostLane& lane, double* out, rodv_stats* st);
   int persistent_blocks(const KernelInfo& k) const;
   std::string device_key() const;
   bool load_tuning(const std::string& path);
@@ -144,6 +162,7 @@ class Engine {
   PinnedMem staging_;
   PinnedMem out_staging_;
   DeviceMem arena_;
+  HostLane lanes_[2];
   std::mutex mu_;
   std::string last_error_;
   bool ready_ = false;
