@@ -26,8 +26,13 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "librodv_pairhmm.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-ftz=true", "-Xcompiler", "-fPIC,-O3",
-                     "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
+# -fmad=false: every fused multiply-add in the device code is an explicit FMA
+# intrinsic; no other multiply and add may be fused by the compiler.  Fusing
+# is not applied uniformly (the two copies of a 2-way unrolled loop can
+# differ), which would make a result depend on the step parity at which its
+# haplotype starts in a chain, i.e. on how the batch was cut.
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-ftz=true", "-fmad=false",
+                     "-Xcompiler", "-fPIC,-O3", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 
 
 def nvcc() -> str:
@@ -77,6 +82,11 @@ def _compile(src: str, force: bool) -> str:
 
 def build(force: bool = False, jobs: int = 0, verbose: bool = True) -> str:
     os.makedirs(BUILD, exist_ok=True)
+    # objects built with other flags are stale
+    stamp = os.path.join(BUILD, "flags.txt")
+    flags = " ".join(NVCC_FLAGS)
+    if not os.path.exists(stamp) or open(stamp).read() != flags:
+        force = True
     srcs = _sources()
     jobs = jobs or min(len(srcs), os.cpu_count() or 4)
     with cf.ThreadPoolExecutor(jobs) as ex:
@@ -88,6 +98,8 @@ def build(force: bool = False, jobs: int = 0, verbose: bool = True) -> str:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
         if verbose:
             print(f"built {LIB}", file=sys.stderr)
+    with open(stamp, "w") as fh:
+        fh.write(flags)
     return LIB
 
 

@@ -32,7 +32,7 @@
 // per-step loads are conflict-free 16-byte vector loads.
 //
 // Precision policies.  F32x2 packs two independent pairs into the two halves
-// of the sm_100 f32x2 instructions (__ffma2_rn / __fadd2_rn / __fmul2_rn), so
+// of the sm_100 f32x2 instructions (fma / add / mul .rn.f32x2), so
 // one warp instruction advances two DP cells.  F64 runs one pair per warp in
 // double precision: it is the rescue pass for pairs whose FP32 result is below
 // the reference's acceptance threshold (MIN_ACCEPTED 1e-28,
@@ -74,13 +74,45 @@ constexpr double kLog10InitF = (double)36.1236000061f;
 constexpr double kLog10InitD = 307.050595577260822;
 constexpr double kDblMin = 2.2250738585072014e-308;  // smallest normal double
 
+// f32x2 arithmetic as PTX with an explicit .rn rounding modifier.  Results
+// must not depend on the step at which a haplotype starts in a sweep (a chain
+// item starts haplotypes at arbitrary steps of a 2-way unrolled loop), so the
+// one product that is summed -- the last row's M into its running sum -- is
+// accumulated with an explicit FMA on every step (acc = fma(t, e, acc)): a
+// multiply followed by an add there was observed to be fused on only one of
+// the two unrolled steps.
+__device__ __forceinline__ unsigned long long f2_bits(float2 v) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(v.x), "f"(v.y));
+  return r;
+}
+__device__ __forceinline__ float2 f2_value(unsigned long long r) {
+  float2 v;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+  return v;
+}
+
 struct F32x2 {
   using V = float2;
   using S = float;
   static constexpr int kSlots = 2;
-  __device__ __forceinline__ static V add(V a, V b) { return __fadd2_rn(a, b); }
-  __device__ __forceinline__ static V mul(V a, V b) { return __fmul2_rn(a, b); }
-  __device__ __forceinline__ static V fma(V a, V b, V c) { return __ffma2_rn(a, b, c); }
+  __device__ __forceinline__ static V add(V a, V b) {
+    unsigned long long r;
+    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+    return f2_value(r);
+  }
+  __device__ __forceinline__ static V mul(V a, V b) {
+    unsigned long long r;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+    return f2_value(r);
+  }
+  __device__ __forceinline__ static V fma(V a, V b, V c) {
+    unsigned long long r;
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;"
+        : "=l"(r)
+        : "l"(f2_bits(a)), "l"(f2_bits(b)), "l"(f2_bits(c)));
+    return f2_value(r);
+  }
   __device__ __forceinline__ static V zero() { return make_float2(0.f, 0.f); }
   __device__ __forceinline__ static V make(S x, S y) { return make_float2(x, y); }
   __device__ __forceinline__ static V shfl_up(V v) {
@@ -309,10 +341,11 @@ struct Forward {
   // One column of this lane's R rows.  (M, I, D)[k] hold the previous
   // column on entry (the left neighbours) and this column on exit; dg is the
   // row above the lane's first row at the previous column, up the same row
-  // at this column.
+  // at this column.  t_last: the last row's M before the emission multiply
+  // (M[R-1] = t_last * e[R-1]), for the running sum of the last row.
   __device__ __forceinline__ static void cells(const V (&e)[R], V up_m, V up_i, V up_d, V& dg_m,
                                                V& dg_i, V& dg_d, V (&M)[R], V (&I)[R], V (&D)[R],
-                                               const Priors& p) {
+                                               const Priors& p, V& t_last) {
     V dm = dg_m, di = dg_i, dd = dg_d, um = up_m, ui = up_i;
 #pragma unroll
     for (int k = 0; k < R; ++k) {
@@ -329,6 +362,7 @@ struct Forward {
       } else {
         M[k] = P::make(P::sx(t) * P::sx(e[k]), P::sy(t) * P::sy(e[k]));
       }
+      if (k == R - 1) t_last = t;
       I[k] = P::fma(p.ii[k], ui, P::mul(p.mi[k], um));
       if (UNIFORM) {
         D[k] = P::fma(p.ddU, oD, P::mul(p.mdU, oM));
@@ -430,9 +464,9 @@ struct Forward {
             up_m = P::zero(); up_i = P::zero(); up_d = init;
           }
         }
-        V e[R];
+        V e[R], t_last;
         load_emission(table, lane, hx[s], kSameHap ? 0u : (uint32_t)hy[s], e);
-        cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr);
+        cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr, t_last);
         if (MULTI && !last && lane == kWarp - 1) {
           const int col = s - (kWarp - 1) + 1;
           if (col >= 1 && col <= (int)sl[0].H) {
@@ -442,7 +476,7 @@ struct Forward {
           }
         }
         if (last) {
-          acc_m = P::add(acc_m, M[R - 1]);
+          acc_m = P::fma(t_last, e[R - 1], acc_m);  // += M[R-1], one rounding
           acc_i = P::add(acc_i, I[R - 1]);
           if (P::kSlots == 2 && !kSameHap && s == nfreeze - 1) {
             frozen_m = P::sy(acc_m);
@@ -553,10 +587,10 @@ struct Forward {
       if (lane == 0) {
         up_m = P::zero(); up_i = P::zero(); up_d = init;
       }
-      V e[R];
+      V e[R], t_last;
       load_emission(table, lane, hx[s], 0u, e);
-      cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr);
-      acc_m = P::add(acc_m, M[R - 1]);
+      cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr, t_last);
+      acc_m = P::fma(t_last, e[R - 1], acc_m);  // += M[R-1], one rounding
       acc_i = P::add(acc_i, I[R - 1]);
       if (s == nxt) {  // this lane just computed a separator column
 #pragma unroll

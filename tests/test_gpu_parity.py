@@ -230,6 +230,33 @@ def test_device_batch_reruns_are_identical(engine):
     db.free()
 
 
+def test_chain_length_does_not_change_results(engine):
+    """A region computed alone (one haplotype per chain item: a small batch)
+    and inside thousands of copies (whole-region chains) gives bitwise the
+    same results, for reads that fill every row of their lanes (length a
+    multiple of 32) and for reads that do not."""
+    rng = np.random.default_rng(12)
+    base = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, 200)]
+    haps = []
+    for k in range(8):
+        h = base[:100 + 60 * (k % 2)].copy()
+        h[rng.random(len(h)) < 0.02] = ord("G")
+        haps.append(h)
+    reads, q, ins, gcp = [], [], [], []
+    for L in (64, 95, 96, 128, 127, 160):
+        st = int(rng.integers(0, 200 - L))
+        reads.append(base[st:st + L].copy())
+        q.append(rng.integers(10, 41, L).astype(np.uint8))
+        ins.append(np.full(L, 45, np.uint8))
+        gcp.append(np.full(L, 10, np.uint8))
+    region = (haps, reads, q, ins, ins, gcp)
+    alone = engine.batch(Batch.from_regions([region]))
+    many = engine.batch(Batch.from_regions([region] * 2000))
+    n = len(alone)
+    assert np.array_equal(many[:n], alone)
+    assert np.array_equal(many[-n:], alone)
+
+
 def test_chunked_host_path_matches_resident(engine):
     """A batch large enough for the pipelined host-buffer path (region ranges
     packed and uploaded while the previous range computes) gives bitwise the
