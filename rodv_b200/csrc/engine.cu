@@ -358,6 +358,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   // ---- read flags (uniform gaps) and class of every read ----
   std::vector<uint8_t>& read_class = plan.read_class;
   read_class.resize(b.num_reads);
+  const HostPriorTables& pt = host_prior_tables();
   parallel_for(b.num_reads, 4096, [&](size_t lo, size_t hi) {
     for (size_t r = lo; r < hi; ++r) {
       const uint64_t off = b.read_offsets[r];
@@ -368,9 +369,15 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       for (uint32_t k = 1; k < n && u; ++k)
         u = (b.ins_quals[off + k] & 127) == i0 && (b.del_quals[off + k] & 127) == d0 &&
             (b.gcp_quals[off + k] & 127) == c0;
-      // The uniform-gap kernels store M/gapm; gcp quality 0 gives gapm = 0,
-      // so such reads take the per-row kernels.
-      read_class[r] = (uint8_t)class_of(n, u && c0 != 0);
+      // Uniform-gap classes: ins, del and gcp constant, ins == del (the
+      // single-pass kernels' scaled form needs mi == md), gcp quality not 0
+      // (gapm = 0), and c = mi*gapm >= 1e-6, so that M/gapm*c -- which the
+      // scaled form keeps -- stays far from the FP32 denormal range for any
+      // likelihood the FP32 pass accepts.  Other reads take the per-row
+      // kernels.
+      const bool uniform = u && c0 != 0 && i0 == d0 &&
+                           (double)pt.ph2pr_f[i0] * (1.0 - (double)pt.ph2pr_f[c0]) >= 1e-6;
+      read_class[r] = (uint8_t)class_of(n, uniform);
     }
   });
 

@@ -219,6 +219,9 @@ struct Forward {
   static constexpr bool kSameHap = Shape::kSameLayout;
   // Single-pass same-haplotype FP32 kernels take chain items.
   static constexpr bool kChain = SAME && !MULTI && P::kSlots == 2;
+  // Chain kernels of the uniform-gap classes use the scaled 5-operation
+  // form (reads of these classes have equal insertion and deletion quality).
+  static constexpr bool kScaled = kChain && UNIFORM;
   static constexpr int kWarpsPerBlock = 4;
   static constexpr int kSmemPerWarp = Shape::kBytesPerWarp + (kChain ? (int)sizeof(ChainMeta) : 0);
 
@@ -252,15 +255,34 @@ struct Forward {
   // the two slots (reads of L[s] rows starting at row word row_off[s]).
   // Rows past a read's end are pass-through rows: emission 0, mi = ii = 1,
   // md = 0 (in the uniform form mi*gapm = gapm, since M~ = M/gapm).
+  //
+  // Scaled form (kScaled; uniform gaps with mi == md).  With c = mi*gapm the
+  // sweep keeps M~ = M/gapm, I^ = I/c, D^ = D/c of a DP whose row 0 holds
+  // D = c*init, so that
+  //   M~ = (e*c) * ((mm/c)*M~_d + I^_d + D^_d)
+  //   I^ = ii*I^_u + M~_u
+  //   D^ = dd*D^_l + M~_l
+  // (5 operations per cell), row 0 is D^ = init, and the read's last row L
+  // uses the emission e*gapm instead of e*c (it holds M~_L/mi), so that the
+  // first pass-through row below it gets I^ = M~_L/mi + I^_L = (M_L + I_L)/c,
+  // the likelihood term of a DP with row 0 = init.  The result is the sum
+  // over columns of M~ + I^ in lane 31's last register.
   __device__ __forceinline__ static void load_rows(const BatchView& b, const uint32_t (&L)[2],
                                                    const uint64_t (&row_off)[2], uint32_t pass,
                                                    int lane, uint4* table, Priors& p) {
     RowPriors<S> u[2];
+    S cs[2] = {S(1), S(1)};  // emission scale of rows before the last (kScaled)
     if (UNIFORM) {  // uniform-gap priors come from the read's first row
       u[0] = row_priors<S>(b.read_rows[row_off[0]], b.tab);
       u[1] = row_priors<S>(b.read_rows[row_off[1]], b.tab);
-      p.mmU = P::make(u[0].mm, u[1].mm);
-      p.mdU = P::make(u[0].md * u[0].gapm, u[1].md * u[1].gapm);
+      if (kScaled) {
+        cs[0] = u[0].mi * u[0].gapm;
+        cs[1] = u[1].mi * u[1].gapm;
+        p.mmU = P::make(u[0].mm / cs[0], u[1].mm / cs[1]);
+      } else {
+        p.mmU = P::make(u[0].mm, u[1].mm);
+        p.mdU = P::make(u[0].md * u[0].gapm, u[1].md * u[1].gapm);
+      }
       p.ddU = P::make(u[0].ii, u[1].ii);
     }
     S* tab = reinterpret_cast<S*>(table);
@@ -274,10 +296,12 @@ struct Forward {
         const uint32_t w = real ? b.read_rows[row_off[s] + row] : 0u;
         const RowPriors<S> rp = row_priors<S>(w, b.tab);
         const uint32_t rc = rw_code(w);
+        const S scale = !kScaled ? S(1) : (row + 1 == L[s] ? u[s].gapm : cs[s]);
 #pragma unroll
         for (int code = 0; code < kN + 1; ++code) {
           const bool hit = (rc == (uint32_t)code) || rc == kN || code == kN;
-          put_emission(tab, s, code, k, lane, real ? (hit ? rp.match : rp.mismatch) : S(0));
+          const S e = hit ? rp.match : rp.mismatch;
+          put_emission(tab, s, code, k, lane, real ? (kScaled ? e * scale : e) : S(0));
         }
         put_emission(tab, s, kSep, k, lane, S(0));
         if (UNIFORM) {
@@ -363,11 +387,16 @@ struct Forward {
         M[k] = P::make(P::sx(t) * P::sx(e[k]), P::sy(t) * P::sy(e[k]));
       }
       if (k == R - 1) t_last = t;
-      I[k] = P::fma(p.ii[k], ui, P::mul(p.mi[k], um));
-      if (UNIFORM) {
-        D[k] = P::fma(p.ddU, oD, P::mul(p.mdU, oM));
+      if (kScaled) {
+        I[k] = P::fma(p.ii[k], ui, um);
+        D[k] = P::fma(p.ddU, oD, oM);
       } else {
-        D[k] = P::fma(p.ii[k], oD, P::mul(p.md[k], oM));
+        I[k] = P::fma(p.ii[k], ui, P::mul(p.mi[k], um));
+        if (UNIFORM) {
+          D[k] = P::fma(p.ddU, oD, P::mul(p.mdU, oM));
+        } else {
+          D[k] = P::fma(p.ii[k], oD, P::mul(p.md[k], oM));
+        }
       }
       dm = oM; di = oI; dd = oD;
       um = M[k]; ui = I[k];
@@ -613,7 +642,10 @@ struct Forward {
       const uint32_t hap = it.hap_start + lane;
       const uint32_t out = it.out_x + (uint32_t)lane * it.stride;
       S res_x, res_y = 0;
-      if (UNIFORM) {
+      if (kScaled) {
+        res_x = a.x + a.z;
+        res_y = a.y + a.w;
+      } else if (UNIFORM) {
         res_x = uniform_gapm(b, it.read_x) * a.x + a.z;
         if (has_y) res_y = uniform_gapm(b, it.read_y) * a.y + a.w;
       } else {
