@@ -590,7 +590,7 @@ def main():
                     help="cpu_baseline: wall seconds of CPU work")
     ap.add_argument("--stream-pool", type=int, default=300,
                     help="streaming (C5): regions in the cycled pool")
-    ap.add_argument("--stream-requests", type=int, default=1200,
+    ap.add_argument("--stream-requests", type=int, default=4000,
                     help="streaming (C5): requests of the saturation run (0: skip C5)")
     ap.add_argument("--stream-verbose", type=int, default=0,
                     help="streaming (C5): service verbosity (2: host time sections)")

@@ -213,12 +213,12 @@ rodv_status rodv_autotune(rodv_engine* engine, const char* cache_path, int32_t f
  * arrive.  rodv_submit_region copies one or more regions (a rodv_batch; the
  * caller's buffers may be reused as soon as it returns) into the service's
  * queue and returns a ticket.  A worker thread puts everything submitted while
- * the GPU was busy into the next device batch (continuous batching over two
- * streams: the next batch is packed and uploaded while the current one
- * computes).  A region's results are bitwise identical whatever it was
+ * the GPU was busy into the next device batch (continuous batching over three
+ * streams: the next batches are packed and uploaded while earlier ones
+ * compute).  A region's results are bitwise identical whatever it was
  * batched with.
  * Admission: opts->device_memory_budget bytes (0 = half of the free device
- * memory) are split between the two batch slots; a request that cannot fit
+ * memory) are split between the three batch slots; a request that cannot fit
  * one slot is refused with RODV_ERR_ADMISSION; rodv_submit_region blocks while
  * opts->max_inflight requests (0 = 4096) are queued or computing.
  * rodv_poll returns RODV_ERR_NOT_READY until the results are available, then

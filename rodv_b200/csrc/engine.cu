@@ -23,8 +23,14 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
+#include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <fstream>
+#include <functional>
+#include <memory>
+#include <mutex>
 #include <random>
 #include <sstream>
 #include <thread>
@@ -49,28 +55,92 @@ struct CodeTable {
 };
 const CodeTable kCodes;
 
+// A process-wide pool of host worker threads for the packer.  parallel_for
+// splits [0, n) into chunks of `grain`; the calling thread and up to
+// (chunks - 1) pool workers take chunks until none is left.  Threads are
+// created once: spawning them per call cost more than packing a small batch.
+class WorkerPool {
+ public:
+  static WorkerPool& get() {
+    static WorkerPool pool;
+    return pool;
+  }
+  unsigned size() const { return (unsigned)threads_.size(); }
+  void submit(std::function<void()> task) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      tasks_.push_back(std::move(task));
+    }
+    cv_.notify_one();
+  }
+
+ private:
+  WorkerPool() {
+    const unsigned n = std::max(1u, std::thread::hardware_concurrency()) - 1;
+    for (unsigned i = 0; i < n; ++i)
+      threads_.emplace_back([this] {
+        for (;;) {
+          std::function<void()> task;
+          {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] { return stop_ || !tasks_.empty(); });
+            if (stop_ && tasks_.empty()) return;
+            task = std::move(tasks_.front());
+            tasks_.pop_front();
+          }
+          task();
+        }
+      });
+  }
+  ~WorkerPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : threads_) t.join();
+  }
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::deque<std::function<void()>> tasks_;
+  std::vector<std::thread> threads_;
+  bool stop_ = false;
+};
+
 template <class F>
 void parallel_for(size_t n, size_t grain, F&& f) {
-  unsigned hw = std::max(1u, std::thread::hardware_concurrency());
   const size_t chunks = (n + grain - 1) / grain;
-  const unsigned nt = (unsigned)std::min<size_t>(hw, chunks);
-  if (nt <= 1) {
+  const unsigned helpers = (unsigned)std::min<size_t>(WorkerPool::get().size(), chunks ? chunks - 1 : 0);
+  if (helpers == 0) {
     if (n) f(0, n);
     return;
   }
-  std::atomic<size_t> next{0};
-  std::vector<std::thread> pool;
-  pool.reserve(nt);
-  for (unsigned t = 0; t < nt; ++t) {
-    pool.emplace_back([&] {
-      for (;;) {
-        const size_t c = next.fetch_add(1);
-        if (c >= chunks) break;
-        f(c * grain, std::min(n, (c + 1) * grain));
+  struct Job {
+    std::atomic<size_t> next{0};
+    std::atomic<unsigned> running{0};
+    std::mutex mu;
+    std::condition_variable cv;
+  };
+  auto job = std::make_shared<Job>();
+  auto work = [job, chunks, grain, n, &f] {
+    for (;;) {
+      const size_t c = job->next.fetch_add(1);
+      if (c >= chunks) break;
+      f(c * grain, std::min(n, (c + 1) * grain));
+    }
+  };
+  job->running = helpers;
+  for (unsigned t = 0; t < helpers; ++t)
+    WorkerPool::get().submit([job, work] {
+      work();
+      if (job->running.fetch_sub(1) == 1) {
+        std::lock_guard<std::mutex> lk(job->mu);
+        job->cv.notify_all();
       }
     });
-  }
-  for (auto& th : pool) th.join();
+  work();
+  std::unique_lock<std::mutex> lk(job->mu);
+  job->cv.wait(lk, [&] { return job->running.load() == 0; });
 }
 
 // Section timer of the packer, printed at verbose level 2.
@@ -253,12 +323,21 @@ rodv_status Engine::init() {
   return RODV_OK;
 }
 
+// Resident blocks of a kernel on the whole device, queried once per kernel
+// (the occupancy query costs more than a launch).
 int Engine::persistent_blocks(const KernelInfo& k) const {
+  {
+    std::lock_guard<std::mutex> lk(occ_mu_);
+    auto it = occ_cache_.find(k.fn);
+    if (it != occ_cache_.end()) return it->second;
+  }
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.threads, k.smem_bytes) !=
           cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
+  std::lock_guard<std::mutex> lk(occ_mu_);
+  occ_cache_[k.fn] = per_sm * num_sms_;
   return per_sm * num_sms_;
 }
 
@@ -806,15 +885,27 @@ static void fill_stats(rodv_stats* st, const PackedPlan& plan, const uint32_t* c
 }
 
 // Host buffers in and out.  A large batch is cut into region ranges that go
-// through two lanes: while one range computes, the host packs the next into
-// the other lane's staging buffer and its upload runs on the copy engine, so
-// packing and transfers hide behind the kernels.  Range sizes start small
+// through three lanes: while ranges compute, the host packs the next into a
+// free lane's staging buffer and its upload runs on the copy engine, so
+// packing and transfers hide behind the kernels (with two lanes the host
+// could only start a range once the range two back had finished, which left
+// the GPU idle between ranges).  Range sizes start small
 // (the first range's packing and upload are not hidden) and double up to
 // kChunkCells cells.  Results do not depend on the cut (a pair's arithmetic
-// depends on its own region only).
-constexpr double kChunkCells = 6e10;
+// depends on its own region only).  Measured on the 10,000-region uneven
+// batch (5.1e11 cells): 3e10-cell ranges 171 ms, 6e10 158 ms, 1.2e11 150 ms
+// per call, against 139 ms of resident compute.
+constexpr double kChunkCells = 1.2e11;
 constexpr double kFirstChunkCells = 4e9;
 constexpr double kMinChunkedCells = 2e10;
+
+// Range sizes, overridable for tuning (RODV_CHUNK_CELLS, RODV_FIRST_CHUNK_CELLS).
+double env_cells(const char* name, double fallback) {
+  const char* v = std::getenv(name);
+  if (!v || !*v) return fallback;
+  const double x = std::atof(v);
+  return x > 0 ? x : fallback;
+}
 
 rodv_status Engine::run_host(const rodv_batch& b, double* out, rodv_stats* st, bool force_fp64) {
   if (!out) return fail(RODV_ERR_INVALID_ARG, "null output");
@@ -834,13 +925,15 @@ rodv_status Engine::run_host(const rodv_batch& b, double* out, rodv_stats* st, b
     for (uint32_t r = 0; r < rg.num_reads; ++r) rs += b.read_lengths[rg.read_start + r];
     cum[g + 1] = cum[g] + hs * rs;
   }
+  static const double chunk_cells = env_cells("RODV_CHUNK_CELLS", kChunkCells);
+  static const double first_cells = env_cells("RODV_FIRST_CHUNK_CELLS", kFirstChunkCells);
   if (cum[G] < kMinChunkedCells || G < 4) return run_host_single(b, out, st, fp64);
   std::vector<uint32_t> bounds{0};
-  double target = std::min(kChunkCells, std::max(kFirstChunkCells, cum[G] / 32));
+  double target = std::min(chunk_cells, std::max(first_cells, cum[G] / 32));
   for (uint32_t g = 1; g < G; ++g) {
     if (cum[g] - cum[bounds.back()] >= target) {
       bounds.push_back(g);
-      target = std::min(kChunkCells, 2 * target);
+      target = std::min(chunk_cells, 2 * target);
     }
   }
   bounds.push_back(G);
@@ -851,6 +944,13 @@ rodv_status Engine::run_host(const rodv_batch& b, double* out, rodv_stats* st, b
 rodv_status Engine::finish_lane(HostLane& l, double* out, rodv_stats* st) {
   l.busy = false;
   RODV_CUDA(cudaEventSynchronize(l.done));
+  if (opt_.verbose >= 2) {
+    float a = 0.f, k0 = 0.f, k1 = 0.f;
+    cudaEventElapsedTime(&a, ev_[3], l.ev[3]);
+    cudaEventElapsedTime(&k0, ev_[3], l.ev[0]);
+    cudaEventElapsedTime(&k1, ev_[3], l.ev[2]);
+    fprintf(stderr, "rodv:   device: upload from %.2f, kernels %.2f-%.2f ms\n", a, k0, k1);
+  }
   const PackedPlan& p = l.plan;
   const uint8_t* h = static_cast<const uint8_t*>(l.out.ptr);
   const uint32_t* counts = reinterpret_cast<const uint32_t*>(h + p.num_pairs * 8);
@@ -879,12 +979,14 @@ rodv_status Engine::finish_lane(HostLane& l, double* out, rodv_stats* st) {
 rodv_status Engine::run_host_chunked(const rodv_batch& b, double* out, rodv_stats* st,
                                      bool fp64, const std::vector<uint32_t>& bounds) {
   const auto t0 = std::chrono::steady_clock::now();
+  const bool timeline = opt_.verbose >= 2;
+  if (timeline) RODV_CUDA(cudaEventRecord(ev_[3], lanes_[0].stream));
   rodv_stats acc{};
   const size_t nchunks = bounds.size() - 1;
   rodv_status result = RODV_OK;
   uint64_t out_off = 0;
   for (size_t k = 0; k < nchunks && result == RODV_OK; ++k) {
-    HostLane& l = lanes_[k & 1];
+    HostLane& l = lanes_[k % kHostLanes];
     if (l.busy) {
       result = finish_lane(l, out, &acc);
       if (result != RODV_OK) break;
@@ -925,8 +1027,12 @@ rodv_status Engine::run_host_chunked(const rodv_batch& b, double* out, rodv_stat
         }
       }
     }
+    const double t_pack0 = ms_since(t0);
     result = pack(v, l.plan, l.staging, fp64);
     if (result != RODV_OK) break;
+    if (timeline)
+      fprintf(stderr, "rodv: range %zu (%u regions, %.2e cells): pack %.2f-%.2f ms\n", k, g1 - g0,
+              (double)l.plan.cells, t_pack0, ms_since(t0));
     const PackedPlan& p = l.plan;
     cudaError_t e = cudaSuccess;
     if (l.arena.bytes < p.total_bytes) e = l.arena.ensure(p.total_bytes + p.total_bytes / 4);
@@ -958,8 +1064,8 @@ rodv_status Engine::run_host_chunked(const rodv_batch& b, double* out, rodv_stat
   }
   // collect what is still in flight, oldest first (on error too: no lane may
   // be left with work that writes into buffers reused by the next call)
-  for (size_t k = nchunks; k < nchunks + 2; ++k) {
-    HostLane& l = lanes_[k & 1];
+  for (size_t k = nchunks; k < nchunks + kHostLanes; ++k) {
+    HostLane& l = lanes_[k % kHostLanes];
     if (!l.busy) continue;
     if (result == RODV_OK) {
       result = finish_lane(l, out, &acc);

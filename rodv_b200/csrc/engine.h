@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/rodv_pairhmm.h"
@@ -113,7 +114,7 @@ class Engine {
   std::mutex& mutex() { return mu_; }
   // One stage of the chunked host-buffer path: a region range packed,
   // uploaded, computed and downloaded on its own stream while the host packs
-  // the next range into the other lane.
+  // the following ranges into the other lanes.
   struct HostLane {
     PackedPlan plan;
     PinnedMem staging, out;
@@ -149,6 +150,8 @@ class Engine {
   bool save_tuning(const std::string& path) const;
 
   rodv_options opt_;
+  mutable std::mutex occ_mu_;
+  mutable std::unordered_map<const void*, int> occ_cache_;  // kernel -> resident blocks
   int device_ = 0;
   int num_sms_ = 0;
   std::string device_name_;
@@ -162,7 +165,8 @@ class Engine {
   PinnedMem staging_;
   PinnedMem out_staging_;
   DeviceMem arena_;
-  HostLane lanes_[2];
+  static constexpr int kHostLanes = 3;
+  HostLane lanes_[kHostLanes];
   std::mutex mu_;
   std::string last_error_;
   bool ready_ = false;

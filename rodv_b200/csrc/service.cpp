@@ -74,7 +74,7 @@ rodv_status Service::init() {
     return st;
   }
   const uint64_t budget = opt_.device_memory_budget ? opt_.device_memory_budget : free_b / 2;
-  slot_budget_ = budget / 2;
+  slot_budget_ = budget / kSlots;
   batch_bytes_ = std::min<uint64_t>(slot_budget_, kBatchBytes);
   max_inflight_ = opt_.max_inflight ? opt_.max_inflight : 4096;
   for (Slot& s : slots_) {
@@ -196,9 +196,10 @@ void Service::worker() {
       std::unique_lock<std::mutex> lk(mu_);
       if (busy.empty()) cv_work_.wait(lk, [&] { return stop_ || !pending_.empty(); });
       if (busy.empty() && pending_.empty() && stop_) break;
-      if (busy.size() < 2 && !pending_.empty()) {
-        // everything queued, up to one slot's budget, goes into the next batch
-        slot = busy.empty() ? 0 : 1 - busy.front();
+      if (busy.size() < (size_t)kSlots && !pending_.empty()) {
+        // everything queued, up to one batch's size, goes into the next batch
+        for (int i = 0; i < kSlots && slot < 0; ++i)
+          if (std::find(busy.begin(), busy.end(), i) == busy.end()) slot = i;
         uint64_t bytes = 0, pairs = 0;
         while (!pending_.empty()) {
           const std::shared_ptr<Request>& r = pending_.front();
@@ -210,9 +211,9 @@ void Service::worker() {
           batch.push_back(r);
           pending_.pop_front();
         }
-      } else if (busy.size() == 1 && pending_.empty()) {
-        // One batch computing and nothing queued: launch a new batch as soon
-        // as something arrives, collect the running one when it is done.
+      } else if (!busy.empty() && busy.size() < (size_t)kSlots && pending_.empty()) {
+        // A slot free and nothing queued: launch a new batch as soon as
+        // something arrives, collect the oldest running one when it is done.
         if (cudaEventQuery(slots_[busy.front()].done) == cudaErrorNotReady) {
           cv_work_.wait_for(lk, std::chrono::microseconds(200),
                             [&] { return stop_ || !pending_.empty(); });

@@ -3,8 +3,8 @@
 // Callers submit regions (one rodv_batch each) at any time and poll or wait
 // for their results.  One worker thread batches whatever has been submitted
 // while the GPU was busy into the next device batch (continuous batching) on
-// two slots, each with its own stream, pinned staging and device arena, so the
-// host packs and uploads batch k+1 while the kernels of batch k run.
+// kSlots slots, each with its own stream, pinned staging and device arena, so
+// the host packs and uploads the next batches while earlier ones compute.
 // Admission: a request larger than a slot's share of the device-memory
 // budget is refused (RODV_ERR_ADMISSION); submit blocks while max_inflight
 // requests are queued or running.  A batch takes queued requests up to a
@@ -79,7 +79,8 @@ class Service {
 
   rodv_options opt_;
   Engine engine_;
-  Slot slots_[2];
+  static constexpr int kSlots = 3;
+  Slot slots_[kSlots];
   uint64_t slot_budget_ = 0;   // largest request (device bytes) a slot admits
   uint64_t batch_bytes_ = 0;   // batches are formed up to this size
   uint32_t max_inflight_ = 0;
