@@ -47,6 +47,33 @@ def build(ref_dir: Optional[str] = None, quiet: bool = True) -> None:
     if os.path.isdir(os.path.join(ref_dir, "src", "core")):
         subprocess.run(["make", "-C", HERE, "ref", f"REF={ref_dir}", "-j8"], check=True,
                        stdout=out)
+        # the reference's scheduler tests linked against the engine's
+        # schedule_pairhmm (needs rodv_b200/librodv_pairhmm.so)
+        if os.path.exists(os.path.join(HERE, "..", "rodv_b200", "librodv_pairhmm.so")):
+            subprocess.run(["make", "-C", HERE, "conformance", f"REF={ref_dir}", "-j8"],
+                           check=True, stdout=out)
+
+
+CONFORMANCE_BIN = os.path.join(HERE, "_ref", "ref_schedule_tests_on_rodv")
+
+
+def write_assemble_log(regions, path: str) -> None:
+    """Writes regions (the assemble fixture's dicts: region, haps, reads, q,
+    ins, del, gcp) in the format AssembleLogParser reads
+    (src/core/test/assemble_log_parser.cpp:13-149)."""
+    with open(path, "w") as fh:
+        for r in regions:
+            fh.write(f"=== Region: {r['region']} ===\n")
+            fh.write(f"Haplotypes: {len(r['haps'])}\nReads: {len(r['reads'])}\n\n")
+            for k, h in enumerate(r["haps"]):
+                fh.write(f"H{k}: {h}\n")
+            fh.write("\n")
+            for k, seq in enumerate(r["reads"]):
+                fh.write(f"R{k}: {seq}\n")
+                for label, key in (("read-qual", "q"), ("read-ins-qual", "ins"),
+                                   ("read-del-qual", "del"), ("gcp", "gcp")):
+                    fh.write(f"  {label}: " + " ".join(str(int(v)) for v in r[key][k]) + "\n")
+            fh.write("\n")
 
 
 def oracle_lib() -> ctypes.CDLL:
