@@ -523,10 +523,13 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   // kChainHaps) that still leave every resident warp of the class's launch
   // (16 per SM at most) two items; a small batch gets short chains (down to
   // one haplotype).
-  const uint64_t target_items = (uint64_t)num_sms_ * 16 * 2;
   for (int c = 0; c < kSinglePassClasses; ++c) {
+    // chain items a warp of this class's kernel sweeps at once
+    const int ipw = forward_kernel_info(Precision::kF32x2, class_rows(c), class_uniform(c),
+                                        false, true, variant_[c]).items_per_warp;
+    const uint64_t target_items = (uint64_t)num_sms_ * 16 * 2 * ipw;
     plan.chain_haps[c] = 1;
-    for (uint32_t cap = kChainHaps; cap >= 1; cap /= 2) {
+    for (uint32_t cap = kChainHaps / ipw; cap >= 1; cap /= 2) {
       uint64_t items = 0;
       for (uint32_t g = 0; g < G; ++g)
         items += (uint64_t)rpairs[(size_t)g * K + c] * ((b.regions[g].num_haps + cap - 1) / cap);
@@ -814,7 +817,8 @@ rodv_status Engine::launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, in
   cl.scratch = a.scratch;
   cl.scratch_cols = plan.scratch_cols;
   cl.error_flags = a.counts + kCtrError;
-  const int need = (int)((n + k.warps_per_block - 1) / k.warps_per_block);
+  const int per_block = k.warps_per_block * k.items_per_warp;
+  const int need = (int)((n + per_block - 1) / per_block);
   int blocks = std::max(1, std::min(persistent_blocks(k), need));
   if (blocks_cap > 0) blocks = std::min(blocks, blocks_cap);
   void* args[] = {&a.view, &cl};

@@ -10,11 +10,11 @@
 
 namespace rodv {
 
-template <class P, int R, bool U, bool MU, bool SAME, int MINB>
+template <class P, int R, bool U, bool MU, bool SAME, int MINB, int GROUP = 32>
 KernelInfo make_info(int variant) {
-  using F = Forward<P, R, U, MU, SAME, MINB>;
+  using F = Forward<P, R, U, MU, SAME, MINB, GROUP>;
   KernelInfo k;
-  k.fn = reinterpret_cast<const void*>(&forward_kernel<P, R, U, MU, SAME, MINB>);
+  k.fn = reinterpret_cast<const void*>(&forward_kernel<P, R, U, MU, SAME, MINB, GROUP>);
   k.threads = F::kWarpsPerBlock * kWarp;
   k.warps_per_block = F::kWarpsPerBlock;
   k.smem_bytes = F::kWarpsPerBlock * F::kSmemPerWarp;
@@ -22,24 +22,31 @@ KernelInfo make_info(int variant) {
   k.multi = MU;
   k.same_hap = SAME || P::kSlots == 1;
   k.chain = F::kChain;
+  k.items_per_warp = F::kGroups;
   k.min_blocks = MINB;
   k.variant = variant;
   return k;
 }
 
 // Same-haplotype FP32 kernels come in kTuneVariants occupancy targets
-// (kVariantMinBlocks); every other kernel has one variant.
+// (kVariantMinBlocks); every other kernel has one variant.  Chain kernels of
+// the classes of reads up to 128 bases (R <= 4) run two 16-lane groups per
+// warp with 2R rows per lane: each lane's per-step overhead (shuffles, code
+// and table loads, row-0 selects) then covers twice the rows.
 template <class P, int R, bool U, bool MU, bool SAME>
 KernelInfo variant_info(int variant) {
   if constexpr (!(std::is_same<P, F32x2>::value && SAME)) {
     (void)variant;
     return make_info<P, R, U, MU, SAME, 1>(0);
   } else {
+    constexpr bool kHalf = !MU && R <= 4;
+    constexpr int RL = kHalf ? 2 * R : R;
+    constexpr int G = kHalf ? 16 : 32;
     switch (variant) {
-      case 0: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[0]>(0);
-      case 1: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[1]>(1);
-      case 2: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[2]>(2);
-      default: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[3]>(3);
+      case 0: return make_info<P, RL, U, MU, SAME, kVariantMinBlocks[0], G>(0);
+      case 1: return make_info<P, RL, U, MU, SAME, kVariantMinBlocks[1], G>(1);
+      case 2: return make_info<P, RL, U, MU, SAME, kVariantMinBlocks[2], G>(2);
+      default: return make_info<P, RL, U, MU, SAME, kVariantMinBlocks[3], G>(3);
     }
   }
 }

@@ -15,6 +15,7 @@ struct KernelInfo {
   bool multi = false;         // sweeps reads longer than 32*R rows in passes
   bool same_hap = false;      // both pairs of an item share the haplotype
   bool chain = false;         // takes ChainItem work (single-pass same-haplotype FP32)
+  int items_per_warp = 1;     // chain items a warp sweeps at once (one per lane group)
   int min_blocks = 1;         // launch-bounds occupancy target (caps registers)
   int variant = 0;
 };

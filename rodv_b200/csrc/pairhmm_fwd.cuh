@@ -203,15 +203,19 @@ struct SlotInfo {
   uint64_t row_off;
 };
 
-// Per-warp shared memory of a chain sweep beyond the emission table: the
-// column of the separator after each haplotype, and lane 31's two running
-// sums (M, I of the last read row; x and y halves) at the end of each one.
+// Per-group shared memory of a chain sweep beyond the emission table: the
+// column of the separator after each haplotype (the last one is the virtual
+// separator just past the chain's end), and the last lane's two running sums
+// (M, I of the last read row; x and y halves) at the end of each haplotype.
 struct ChainMeta {
   float4 acc[kChainHaps];
-  uint32_t sep[kChainHaps];
+  uint32_t sep[kChainHaps + 4];  // kChainHaps + 1 used; padded to 16 bytes
 };
 
-template <class P, int R, bool UNIFORM, bool MULTI, bool SAME, int MINB>
+// GROUP: lanes per wavefront.  32 (the whole warp) for every kernel but the
+// chain kernels of short reads, which split the warp into two 16-lane groups
+// with twice the rows per lane, each sweeping its own chain item.
+template <class P, int R, bool UNIFORM, bool MULTI, bool SAME, int MINB, int GROUP = 32>
 struct Forward {
   using V = typename P::V;
   using S = typename P::S;
@@ -219,11 +223,27 @@ struct Forward {
   static constexpr bool kSameHap = Shape::kSameLayout;
   // Single-pass same-haplotype FP32 kernels take chain items.
   static constexpr bool kChain = SAME && !MULTI && P::kSlots == 2;
+  static constexpr int kGroup = GROUP;
+  static constexpr int kGroups = kWarp / GROUP;       // chain items per warp
+  static constexpr int kGroupHaps = kChainHaps / kGroups;  // haplotypes per chain item
+  static_assert(GROUP == 32 || kChain, "lane groups are for chain kernels only");
   // Chain kernels of the uniform-gap classes use the scaled 5-operation
   // form (reads of these classes have equal insertion and deletion quality).
   static constexpr bool kScaled = kChain && UNIFORM;
   static constexpr int kWarpsPerBlock = 4;
-  static constexpr int kSmemPerWarp = Shape::kBytesPerWarp + (kChain ? (int)sizeof(ChainMeta) : 0);
+  static constexpr int kSmemPerWarp =
+      Shape::kBytesPerWarp + (kChain ? kGroups * (int)sizeof(ChainMeta) : 0);
+
+  // Shuffles within a lane group (the row above comes from the previous lane
+  // of the same group).
+  __device__ __forceinline__ static V group_shfl_up(V v) {
+    if constexpr (P::kSlots == 2) {
+      return P::make(__shfl_up_sync(kFullMask, P::sx(v), 1, GROUP),
+                     __shfl_up_sync(kFullMask, P::sy(v), 1, GROUP));
+    } else {
+      return P::shfl_up(v);
+    }
+  }
 
   // Boundary row written by lane 31 of one pass and read by lane 0 of the next.
   struct BoundaryCell {
@@ -251,8 +271,9 @@ struct Forward {
     }
   }
 
-  // Emission tables and priors for read rows pass*32R + lane*R + [0, R) of
-  // the two slots (reads of L[s] rows starting at row word row_off[s]).
+  // Emission tables and priors of this lane (table slot `lane`) for read rows
+  // first_row + [0, R) of the two slots (reads of L[s] rows starting at row
+  // word row_off[s]).
   // Rows past a read's end are pass-through rows: emission 0, mi = ii = 1,
   // md = 0 (in the uniform form mi*gapm = gapm, since M~ = M/gapm).
   //
@@ -268,8 +289,9 @@ struct Forward {
   // the likelihood term of a DP with row 0 = init.  The result is the sum
   // over columns of M~ + I^ in lane 31's last register.
   __device__ __forceinline__ static void load_rows(const BatchView& b, const uint32_t (&L)[2],
-                                                   const uint64_t (&row_off)[2], uint32_t pass,
-                                                   int lane, uint4* table, Priors& p) {
+                                                   const uint64_t (&row_off)[2],
+                                                   uint32_t first_row, int lane, uint4* table,
+                                                   Priors& p) {
     RowPriors<S> u[2];
     S cs[2] = {S(1), S(1)};  // emission scale of rows before the last (kScaled)
     if (UNIFORM) {  // uniform-gap priors come from the read's first row
@@ -288,7 +310,7 @@ struct Forward {
     S* tab = reinterpret_cast<S*>(table);
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-      const uint32_t row = pass * (kWarp * R) + lane * R + k;  // 0-based read row
+      const uint32_t row = first_row + k;  // 0-based read row
       S mmv[2], gv[2], miv[2], iiv[2], mdv[2];
 #pragma unroll
       for (int s = 0; s < P::kSlots; ++s) {
@@ -470,7 +492,7 @@ struct Forward {
     for (uint32_t pass = 0; pass < passes; ++pass) {
       const bool last = (pass + 1 == passes);
       Priors pr;
-      load_rows(b, L, row_off, pass, lane, table, pr);
+      load_rows(b, L, row_off, pass * (kWarp * R) + lane * R, lane, table, pr);
 
       V M[R], I[R], D[R];
 #pragma unroll
@@ -547,100 +569,120 @@ struct Forward {
   //   I = 0 there (the column above it is 0 down from row 0),
   //   D is set to 0 by the lane after it computes the separator column.
   // So every haplotype sees the reference's column-0 boundary, and the
-  // wavefront fills and drains once per chain instead of once per pair.
+  // wavefront fills and drains once per chain instead of once per pair.  A
+  // virtual separator just past the chain's last haplotype (the packed layout
+  // has a separator code after every haplotype) ends the last haplotype's
+  // sums the same way, so the two lane groups of a short-read warp can sweep
+  // chains of different lengths in the same loop.
   // Row 0 uses one scaling constant for the whole chain, 2^120/norm_len
   // (norm_len: the region's longest haplotype, so no value exceeds the
   // reference's); the DP is linear in it, so haplotype i's result is
   // rescaled by (2^120/H_i)/(2^120/norm_len) in FP64 before the acceptance
   // test and log10.
-  __device__ static void run_chain(const BatchView& b, const ClassLaunch& c, uint32_t item,
-                                   int lane, uint4* table) {
-    ChainMeta* meta = reinterpret_cast<ChainMeta*>(table + Shape::kBytesPerWarp / 16);
-    const ChainItem it = static_cast<const ChainItem*>(c.work)[item];
+  // `items`: the chain items of this warp, one per lane group; `count`: how
+  // many of them exist (a group without one repeats the first and writes
+  // nothing).
+  __device__ static void run_chain(const BatchView& b, const ClassLaunch& c, uint32_t first,
+                                   uint32_t count, int lane, uint4* table) {
+    const int grp = lane / GROUP;            // lane group
+    const int gl = lane & (GROUP - 1);       // lane within its group
+    const bool active = first + (uint32_t)grp < count;
+    ChainMeta* meta =
+        reinterpret_cast<ChainMeta*>(table + Shape::kBytesPerWarp / 16) + grp;
+    const ChainItem it =
+        static_cast<const ChainItem*>(c.work)[first + (active ? (uint32_t)grp : 0u)];
     const bool has_y = it.read_y != kNoPair;
     const uint32_t n = it.num_haps;
     const ReadDesc rx = b.reads[it.read_x];
     const ReadDesc ry = b.reads[has_y ? it.read_y : it.read_x];
-    // lane i holds haplotype i's length and code offset
+    // lane gl of a group holds haplotype gl's length and code offset
     uint32_t hl = 0;
     uint64_t co = 0;
-    if ((uint32_t)lane < n && n <= (uint32_t)kChainHaps) {
-      const HapDesc hd = b.haps[it.hap_start + lane];
+    if ((uint32_t)gl < n && n <= (uint32_t)kGroupHaps) {
+      const HapDesc hd = b.haps[it.hap_start + gl];
       hl = hd.len;
       co = hd.code_off;
     }
-    const uint64_t co_next = __shfl_down_sync(kFullMask, co, 1);
-    const bool bad_hap = (uint32_t)lane < n && (hl == 0 || ((uint32_t)lane + 1 < n &&
-                                                            co_next != co + hl + 1));
+    const uint64_t co_next = __shfl_down_sync(kFullMask, co, 1, GROUP);
+    const bool bad_hap = (uint32_t)gl < n && (hl == 0 || ((uint32_t)gl + 1 < n &&
+                                                          co_next != co + hl + 1));
     const uint32_t Lmax = rx.len > ry.len ? rx.len : ry.len;
-    if (__any_sync(kFullMask, bad_hap || hl > it.norm_len) || n == 0 ||
-        n > (uint32_t)kChainHaps || rx.len == 0 || ry.len == 0 || Lmax > (uint32_t)(kWarp * R)) {
+    const bool bad = bad_hap || hl > it.norm_len || n == 0 || n > (uint32_t)kGroupHaps ||
+                     rx.len == 0 || ry.len == 0 || Lmax > (uint32_t)(GROUP * R);
+    if (__any_sync(kFullMask, bad)) {
       if (lane == 0) atomicOr(c.error_flags, kErrChain);
       return;
     }
-    // end column (exclusive) + 1 of haplotype `lane` in the chain's columns
-    uint32_t endc = (uint32_t)lane < n ? hl + 1 : 0;
+    // end column (exclusive) + 1 of haplotype gl in the chain's columns
+    uint32_t endc = (uint32_t)gl < n ? hl + 1 : 0;
 #pragma unroll
-    for (int d = 1; d < kWarp; d *= 2) {
-      const uint32_t v = __shfl_up_sync(kFullMask, endc, d);
-      if (lane >= d) endc += v;
+    for (int d = 1; d < GROUP; d *= 2) {
+      const uint32_t v = __shfl_up_sync(kFullMask, endc, d, GROUP);
+      if (gl >= d) endc += v;
     }
     constexpr uint32_t kNever = 0x40000000u;  // beyond every chain's last step
-    meta->sep[lane] = ((uint32_t)lane + 1 < n) ? endc - 1 : kNever;
-    const uint32_t ncols = __shfl_sync(kFullMask, endc, (int)n - 1) - 1;  // sum H + n - 1
-    const uint64_t co0 = __shfl_sync(kFullMask, co, 0);
+    // separator after haplotype gl (the last one: the virtual end separator)
+    meta->sep[gl] = ((uint32_t)gl < n) ? endc - 1 : kNever;  // kGroupHaps == GROUP
+    if (gl == 0) meta->sep[kGroupHaps] = kNever;
+    const uint32_t ncols = __shfl_sync(kFullMask, endc, (int)n - 1, GROUP) - 1;  // sum H + n - 1
+    uint32_t span = ncols;  // columns of the longer chain of the warp
+    if (kGroups > 1) span = max(span, __shfl_xor_sync(kFullMask, span, GROUP));
+    const uint64_t co0 = __shfl_sync(kFullMask, co, 0, GROUP);
     const S init_s = P::init_const() / (S)it.norm_len;
     const V init = P::make(init_s, init_s);
     const uint32_t L[2] = {rx.len, ry.len};
     const uint64_t row_off[2] = {rx.row_off, ry.row_off};
     Priors pr;
-    load_rows(b, L, row_off, 0, lane, table, pr);
+    load_rows(b, L, row_off, (uint32_t)(gl * R), lane, table, pr);
     __syncwarp();
 
     V M[R], I[R], D[R];
 #pragma unroll
     for (int k = 0; k < R; ++k) M[k] = I[k] = D[k] = P::zero();
     V dg_m = P::zero(), dg_i = P::zero(), dg_d = P::zero();
-    if (lane == 0) dg_d = init;
-    const uint8_t* hx = b.hap_codes + co0 - lane;
+    if (gl == 0) dg_d = init;
+    const uint8_t* hx = b.hap_codes + co0 - gl;
     uint32_t hi = 0;                          // this lane's haplotype in the chain
-    int nxt = (int)meta->sep[0] + lane;       // step at which this lane is at the next separator
+    int nxt = (int)meta->sep[0] + gl;         // step at which this lane is at the next separator
     V acc_m = P::zero(), acc_i = P::zero();
-    const int nsteps = (int)ncols + kWarp - 1;
+    // through the virtual end separator of the longer chain, for the last lane
+    const int nsteps = (int)span + GROUP;
+    // A lane of the shorter chain of a two-group warp keeps stepping past its
+    // virtual end separator (column ncols) with nothing left to compute; its
+    // code index stays clamped there so it reads no byte past its chain.
+    const int last_s = (int)ncols + gl;
 
 #pragma unroll 2
     for (int s = 0; s < nsteps; ++s) {
-      V up_m = P::shfl_up(M[R - 1]);
-      V up_i = P::shfl_up(I[R - 1]);
-      V up_d = P::shfl_up(D[R - 1]);
-      if (lane == 0) {
+      V up_m = group_shfl_up(M[R - 1]);
+      V up_i = group_shfl_up(I[R - 1]);
+      V up_d = group_shfl_up(D[R - 1]);
+      if (gl == 0) {
         up_m = P::zero(); up_i = P::zero(); up_d = init;
       }
       V e[R], t_last;
-      load_emission(table, lane, hx[s], 0u, e);
+      load_emission(table, lane, hx[kGroups > 1 ? min(s, last_s) : s], 0u, e);
       cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr, t_last);
       acc_m = P::fma(t_last, e[R - 1], acc_m);  // += M[R-1], one rounding
       acc_i = P::add(acc_i, I[R - 1]);
       if (s == nxt) {  // this lane just computed a separator column
 #pragma unroll
         for (int k = 0; k < R; ++k) D[k] = P::zero();
-        if (lane == kWarp - 1) {
+        if (gl == GROUP - 1) {
           meta->acc[hi] = make_float4(P::sx(acc_m), P::sy(acc_m), P::sx(acc_i), P::sy(acc_i));
           acc_m = P::zero();
           acc_i = P::zero();
         }
         ++hi;
-        nxt = (int)meta->sep[hi] + lane;
+        nxt = (int)meta->sep[hi] + gl;
       }
     }
-    if (lane == kWarp - 1)
-      meta->acc[n - 1] = make_float4(P::sx(acc_m), P::sy(acc_m), P::sx(acc_i), P::sy(acc_i));
     __syncwarp();
-    if ((uint32_t)lane < n) {
-      const float4 a = meta->acc[lane];
+    if (active && (uint32_t)gl < n) {
+      const float4 a = meta->acc[gl];
       const double ratio = (double)(P::init_const() / (S)hl) / (double)init_s;
-      const uint32_t hap = it.hap_start + lane;
-      const uint32_t out = it.out_x + (uint32_t)lane * it.stride;
+      const uint32_t hap = it.hap_start + gl;
+      const uint32_t out = it.out_x + (uint32_t)gl * it.stride;
       S res_x, res_y = 0;
       if (kScaled) {
         res_x = a.x + a.z;
@@ -681,11 +723,11 @@ struct Forward {
   }
 };
 
-template <class P, int R, bool UNIFORM, bool MULTI, bool SAME, int MINB>
-__global__ void __launch_bounds__(Forward<P, R, UNIFORM, MULTI, SAME, MINB>::kWarpsPerBlock * kWarp,
-                                  MINB)
+template <class P, int R, bool UNIFORM, bool MULTI, bool SAME, int MINB, int GROUP = 32>
+__global__ void __launch_bounds__(
+    Forward<P, R, UNIFORM, MULTI, SAME, MINB, GROUP>::kWarpsPerBlock * kWarp, MINB)
     forward_kernel(BatchView b, ClassLaunch c) {
-  using F = Forward<P, R, UNIFORM, MULTI, SAME, MINB>;
+  using F = Forward<P, R, UNIFORM, MULTI, SAME, MINB, GROUP>;
   extern __shared__ uint4 smem[];
   const int lane = threadIdx.x & (kWarp - 1);
   const int warp = threadIdx.x / kWarp;
@@ -694,11 +736,11 @@ __global__ void __launch_bounds__(Forward<P, R, UNIFORM, MULTI, SAME, MINB>::kWa
   const uint32_t n = c.work_count ? *c.work_count : c.static_count;
   for (;;) {
     uint32_t item = 0;
-    if (lane == 0) item = atomicAdd(c.counter, 1u);
+    if (lane == 0) item = atomicAdd(c.counter, (uint32_t)F::kGroups);
     item = __shfl_sync(kFullMask, item, 0);
     if (item >= n) break;
     if constexpr (F::kChain)
-      F::run_chain(b, c, item, lane, table);
+      F::run_chain(b, c, item, n, lane, table);
     else
       F::run_item(b, c, item, lane, gwarp, table);
   }

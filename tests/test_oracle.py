@@ -87,3 +87,26 @@ def test_oracle_matches_reference_library_on_uneven_sample():
     ref = oracle.ref_schedule(b)
     got = oracle.batch_log10(b, oracle.REFERENCE)
     assert np.abs(got - ref).max() < 1e-5
+
+
+def test_assemble_log_reader_round_trips_the_logged_regions(tmp_path):
+    """rodv_b200.assemble_log reads roDV's assemble-log format: the 8 chrY
+    regions written in that format come back as the same batch."""
+    from conftest import assemble_batch, load_assemble
+    from rodv_b200 import assemble_log
+    regs = load_assemble()
+    path = tmp_path / "pairhmm_debug.txt"
+    oracle.write_assemble_log(regs, str(path))
+    parsed = assemble_log.parse_file(str(path))
+    assert [p.name for p in parsed] == [r["region"] for r in regs]
+    assert all(p.skipped_reads == 0 for p in parsed)
+    b = assemble_log.to_batch(parsed)
+    ref_b, _ = assemble_batch()
+    for f in ("regions", "hap_bases", "hap_lengths", "read_bases", "base_quals", "ins_quals",
+              "del_quals", "gcp_quals", "read_lengths"):
+        assert np.array_equal(getattr(b, f), getattr(ref_b, f)), f
+    # a read whose quality line is short is dropped and counted
+    text = path.read_text().replace("  gcp: 10 10 10 10 10 10 10 10 10 10 10 10 10 10 10\n",
+                                    "  gcp: 10 10\n", 1)
+    bad = assemble_log.parse_lines(text.splitlines(keepends=True))
+    assert bad[0].skipped_reads == 1 and len(bad[0].reads) == len(parsed[0].reads) - 1
