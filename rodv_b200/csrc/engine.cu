@@ -191,9 +191,9 @@ ArenaView arena_view(const PackedPlan& p, uint8_t* base, const PriorTables& tab)
 // measured best for each rows-per-lane value on B200.
 int default_variant(int cls) {
   const int R = class_rows(cls);
-  if (class_multi(cls) || R >= 3) return 0;  // 4 blocks/SM: up to 128 registers
-  if (R == 2) return 2;                      // 6 blocks/SM: up to 80 registers
-  return 3;                                  // 8 blocks/SM: up to 64 registers
+  if (class_multi(cls) || R >= 3) return 0;  // one chain per warp, 4 blocks/SM (128 registers)
+  if (R == 2) return 4;                      // two 16-lane groups, 4 blocks/SM
+  return 6;                                  // two 16-lane groups, 6 blocks/SM (80 registers)
 }
 
 }  // namespace
@@ -307,7 +307,7 @@ rodv_status Engine::init() {
     for (int p = 0; p < 3; ++p)
       for (int v = 0; v < kTuneVariants; ++v) {
         const Precision pr = p == 2 ? Precision::kF64 : Precision::kF32x2;
-        if (v > 0 && forward_kernel_variants(pr, p == 0) == 1) continue;
+        if (v >= forward_kernel_variants(pr, p == 0, class_rows(c), class_multi(c))) continue;
         const KernelInfo k =
             forward_kernel_info(pr, class_rows(c), class_uniform(c), class_multi(c), p == 0, v);
         if (k.fn && k.smem_bytes > 48 * 1024)
@@ -523,10 +523,11 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   // kChainHaps) that still leave every resident warp of the class's launch
   // (16 per SM at most) two items; a small batch gets short chains (down to
   // one haplotype).
+  for (int c = 0; c < kNumClasses; ++c) plan.variant[c] = variant_[c];
   for (int c = 0; c < kSinglePassClasses; ++c) {
     // chain items a warp of this class's kernel sweeps at once
     const int ipw = forward_kernel_info(Precision::kF32x2, class_rows(c), class_uniform(c),
-                                        false, true, variant_[c]).items_per_warp;
+                                        false, true, plan.variant[c]).items_per_warp;
     const uint64_t target_items = (uint64_t)num_sms_ * 16 * 2 * ipw;
     plan.chain_haps[c] = 1;
     for (uint32_t cap = kChainHaps / ipw; cap >= 1; cap /= 2) {
@@ -638,7 +639,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       for (int p = 0; p < 3; ++p)
         for (int v = 0; v < kTuneVariants; ++v) {
           const Precision pr = p == 2 ? Precision::kF64 : Precision::kF32x2;
-          if (v > 0 && forward_kernel_variants(pr, p == 0) == 1) continue;
+          if (v >= forward_kernel_variants(pr, p == 0, kMaxRowsPerLane, true)) continue;
           const KernelInfo k = forward_kernel_info(pr, kMaxRowsPerLane, u != 0, true, p == 0, v);
           warps = std::max(warps, persistent_blocks(k) * k.warps_per_block);
         }
@@ -841,7 +842,7 @@ rodv_status Engine::launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stat
     for (int c = 0; c < kNumClasses; ++c) {
       for (int same = 1; same >= 0; --same) {
         if (!(same ? plan.same_items[c] : plan.diff_items[c])) continue;
-        rodv_status s = launch_fp32_class(plan, dbase, c, same != 0, variant_[c], 0, stream);
+        rodv_status s = launch_fp32_class(plan, dbase, c, same != 0, plan.variant[c], 0, stream);
         if (s != RODV_OK) return s;
         ++launches;
       }
@@ -1392,7 +1393,8 @@ rodv_status Engine::autotune(const char* cache_path, int force, int32_t* variant
     const uint32_t* counts = reinterpret_cast<const uint32_t*>(d + db->plan.off_counts);
     float best_ms = 1e30f;
     int best_v = variant_[c];
-    for (int v = 0; v < kTuneVariants; ++v) {
+    const int nvar = forward_kernel_variants(Precision::kF32x2, true, R, multi);
+    for (int v = 0; v < nvar; ++v) {
       float vbest = 1e30f;
       for (int rep = 0; rep < 3; ++rep) {
         RODV_CUDA(cudaMemsetAsync((void*)counts, 0, kCountWords * 4, stream_));

@@ -71,6 +71,7 @@ struct PackedPlan {
   uint32_t same_items[kNumClasses] = {};
   uint32_t diff_items[kNumClasses] = {};   // FP32 two-haplotype items (multi-pass leftovers)
   uint32_t chain_haps[kNumClasses] = {};   // haplotypes per chain item (single-pass classes)
+  int variant[kNumClasses] = {};           // kernel variant per class the items were packed for
   uint32_t pairs[kNumClasses] = {};        // pairs per class (FP64 list capacity)
   size_t off_hap_codes = 0, off_read_rows = 0, off_haps = 0, off_reads = 0;
   size_t off_same[kNumClasses] = {};

@@ -28,25 +28,33 @@ KernelInfo make_info(int variant) {
   return k;
 }
 
-// Same-haplotype FP32 kernels come in kTuneVariants occupancy targets
-// (kVariantMinBlocks); every other kernel has one variant.  Chain kernels of
-// the classes of reads up to 128 bases (R <= 4) run two 16-lane groups per
-// warp with 2R rows per lane: each lane's per-step overhead (shuffles, code
-// and table loads, row-0 selects) then covers twice the rows.
+// Same-haplotype FP32 kernels come in occupancy targets (kVariantMinBlocks);
+// the chain kernels of reads up to 128 bases (R <= 4) also in a lane-grouped
+// form: two 16-lane groups per warp, each sweeping its own chain item with
+// 2R rows per lane, so that each lane's per-step overhead (shuffles, code and
+// table loads, row-0 selects) covers twice the rows (faster at R <= 2 on B200,
+// slower at R >= 3, where the longer per-step dependency chain shows; the
+// autotuner picks).  Every other kernel has one variant.
 template <class P, int R, bool U, bool MU, bool SAME>
 KernelInfo variant_info(int variant) {
   if constexpr (!(std::is_same<P, F32x2>::value && SAME)) {
     (void)variant;
     return make_info<P, R, U, MU, SAME, 1>(0);
   } else {
-    constexpr bool kHalf = !MU && R <= 4;
-    constexpr int RL = kHalf ? 2 * R : R;
-    constexpr int G = kHalf ? 16 : 32;
+    if constexpr (!MU && R <= kMaxGroupedRows) {
+      switch (variant) {
+        case 4: return make_info<P, 2 * R, U, MU, SAME, kVariantMinBlocks[4], 16>(4);
+        case 5: return make_info<P, 2 * R, U, MU, SAME, kVariantMinBlocks[5], 16>(5);
+        case 6: return make_info<P, 2 * R, U, MU, SAME, kVariantMinBlocks[6], 16>(6);
+        case 7: return make_info<P, 2 * R, U, MU, SAME, kVariantMinBlocks[7], 16>(7);
+        default: break;
+      }
+    }
     switch (variant) {
-      case 0: return make_info<P, RL, U, MU, SAME, kVariantMinBlocks[0], G>(0);
-      case 1: return make_info<P, RL, U, MU, SAME, kVariantMinBlocks[1], G>(1);
-      case 2: return make_info<P, RL, U, MU, SAME, kVariantMinBlocks[2], G>(2);
-      default: return make_info<P, RL, U, MU, SAME, kVariantMinBlocks[3], G>(3);
+      case 0: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[0]>(0);
+      case 1: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[1]>(1);
+      case 2: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[2]>(2);
+      default: return make_info<P, R, U, MU, SAME, kVariantMinBlocks[3]>(3);
     }
   }
 }

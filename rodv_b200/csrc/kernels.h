@@ -20,20 +20,28 @@ struct KernelInfo {
   int variant = 0;
 };
 
-// Occupancy targets of the tunable (same-haplotype FP32) kernels.
-constexpr int kTuneVariants = 4;
-constexpr int kVariantMinBlocks[kTuneVariants] = {4, 5, 6, 8};
+// Variants of the tunable (same-haplotype FP32) kernels: an occupancy target
+// (blocks per SM, which caps registers) and, for the chain kernels of reads
+// up to 128 bases (R <= 4), the lane grouping: variants 0-3 sweep one chain
+// item per warp with R rows per lane, 4-7 two items per warp in 16-lane
+// groups with 2R rows per lane.
+constexpr int kTuneVariants = 8;
+constexpr int kOccupancyTargets = 4;
+constexpr int kVariantMinBlocks[kTuneVariants] = {4, 5, 6, 8, 4, 5, 6, 8};
+constexpr int kMaxGroupedRows = 4;  // classes with R <= 4 have the grouped variants
 
 // Forward kernel for one work class.  rows_per_lane in 1..8; multi kernels
 // always use 8 rows per lane.  same: FP32 items whose reads share the
 // haplotypes -- ChainItem for single-pass classes, SameItem for multi-pass
 // ones; !same: DiffItem (multi-pass only; fn is null for a single-pass class).
-// FP64 kernels take PairRef lists.  variant < kTuneVariants selects the
-// occupancy target of same-haplotype FP32 kernels.
+// FP64 kernels take PairRef lists.  variant < forward_kernel_variants(...)
+// selects the variant of same-haplotype FP32 kernels.
 KernelInfo forward_kernel_info(Precision prec, int rows_per_lane, bool uniform, bool multi,
                                bool same = true, int variant = 0);
-inline int forward_kernel_variants(Precision prec, bool same) {
-  return (prec == Precision::kF32x2 && same) ? kTuneVariants : 1;
+inline int forward_kernel_variants(Precision prec, bool same, int rows_per_lane = 8,
+                                   bool multi = true) {
+  if (prec != Precision::kF32x2 || !same) return 1;
+  return (!multi && rows_per_lane <= kMaxGroupedRows) ? kTuneVariants : kOccupancyTargets;
 }
 
 // Peak microbenchmarks: kind 0 = FP32 FFMA, 1 = FP32x2 FFMA2, 2 = FP64 DFMA.

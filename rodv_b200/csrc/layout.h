@@ -154,6 +154,7 @@ enum ErrorFlag : uint32_t {
   kErrBadLength = 1u,   // a pair with zero or over-limit length reached a kernel
   kErrPassLimit = 2u,   // a read longer than the pass limit reached a kernel
   kErrChain = 4u,       // a chain item with no haplotypes
+  kErrNonFinite = 8u,   // a likelihood came out NaN or infinite (an arithmetic fault)
 };
 
 }  // namespace rodv

@@ -227,9 +227,11 @@ struct Forward {
   static constexpr int kGroups = kWarp / GROUP;       // chain items per warp
   static constexpr int kGroupHaps = kChainHaps / kGroups;  // haplotypes per chain item
   static_assert(GROUP == 32 || kChain, "lane groups are for chain kernels only");
-  // Chain kernels of the uniform-gap classes use the scaled 5-operation
-  // form (reads of these classes have equal insertion and deletion quality).
-  static constexpr bool kScaled = kChain && UNIFORM;
+  // FP32 kernels of the uniform-gap classes use the scaled 5-operation form
+  // (reads of these classes have equal insertion and deletion quality).  The
+  // FP64 kernels keep the unscaled form: they have no fallback, and the scaled
+  // form would lose precision just above the reference's FP64 underflow limit.
+  static constexpr bool kScaled = UNIFORM && P::kSlots == 2;
   static constexpr int kWarpsPerBlock = 4;
   static constexpr int kSmemPerWarp =
       Shape::kBytesPerWarp + (kChain ? kGroups * (int)sizeof(ChainMeta) : 0);
@@ -283,11 +285,14 @@ struct Forward {
   //   M~ = (e*c) * ((mm/c)*M~_d + I^_d + D^_d)
   //   I^ = ii*I^_u + M~_u
   //   D^ = dd*D^_l + M~_l
-  // (5 operations per cell), row 0 is D^ = init, and the read's last row L
-  // uses the emission e*gapm instead of e*c (it holds M~_L/mi), so that the
-  // first pass-through row below it gets I^ = M~_L/mi + I^_L = (M_L + I_L)/c,
-  // the likelihood term of a DP with row 0 = init.  The result is the sum
-  // over columns of M~ + I^ in lane 31's last register.
+  // (5 operations per cell) and row 0 is D^ = init.  The first pass-through
+  // row below the read's last row L takes ii = mi instead of 1, so it holds
+  // mi*I^_L + M~_L = (M_L + I_L)/gapm, and the rows below it copy that value
+  // down.  The likelihood term of a DP with row 0 = init is (M_L + I_L)/c, so
+  // the result is (sum of that row)/mi when lane 31's last register is a
+  // pass-through row, and sum(M~_L)/mi + sum(I^_L) when it is row L itself.
+  // (Scaling row L by 1/mi instead would make the next row's (mm/c)*M~
+  // overflow for likely pairs on short haplotypes.)
   __device__ __forceinline__ static void load_rows(const BatchView& b, const uint32_t (&L)[2],
                                                    const uint64_t (&row_off)[2],
                                                    uint32_t first_row, int lane, uint4* table,
@@ -318,7 +323,7 @@ struct Forward {
         const uint32_t w = real ? b.read_rows[row_off[s] + row] : 0u;
         const RowPriors<S> rp = row_priors<S>(w, b.tab);
         const uint32_t rc = rw_code(w);
-        const S scale = !kScaled ? S(1) : (row + 1 == L[s] ? u[s].gapm : cs[s]);
+        const S scale = kScaled ? cs[s] : S(1);
 #pragma unroll
         for (int code = 0; code < kN + 1; ++code) {
           const bool hit = (rc == (uint32_t)code) || rc == kN || code == kN;
@@ -326,7 +331,9 @@ struct Forward {
           put_emission(tab, s, code, k, lane, real ? (kScaled ? e * scale : e) : S(0));
         }
         put_emission(tab, s, kSep, k, lane, S(0));
-        if (UNIFORM) {
+        if (kScaled) {
+          iiv[s] = real ? u[s].ii : (row == L[s] ? u[s].mi : S(1));
+        } else if (UNIFORM) {
           miv[s] = real ? u[s].mi * u[s].gapm : u[s].gapm;
           iiv[s] = real ? u[s].ii : S(1);
         } else {
@@ -451,6 +458,22 @@ struct Forward {
     return S(1) - __ldg(Tables<S>::ph2pr(b.tab) + rw_gcp(w));
   }
 
+  // The scaled form's likelihood from the last register's column sums of
+  // M~ (acc_m) and I^ (acc_i); rows: the rows the sweep held for the read.
+  // accept_min: the FP32 acceptance bound for it.  The scaled sweep keeps M
+  // about c = mi*gapm times smaller than the reference's FP32 sweep, so its
+  // bound is 1e-28/c: an accepted result keeps the reference's headroom above
+  // the FP32 denormal range (below the bound, the pair goes to FP64).
+  __device__ __forceinline__ static double scaled_result(const BatchView& b, uint32_t read,
+                                                         uint32_t len, uint32_t rows, S acc_m,
+                                                         S acc_i, double* accept_min) {
+    const uint32_t w = b.read_rows[b.reads[read].row_off];
+    const double mi = (double)__ldg(Tables<S>::ph2pr(b.tab) + rw_ins(w));
+    const double gapm = 1.0 - (double)__ldg(Tables<S>::ph2pr(b.tab) + rw_gcp(w));
+    *accept_min = (double)kMinAcceptedF / (mi * gapm);
+    return len < rows ? (double)acc_i / mi : (double)acc_m / mi + (double)acc_i;
+  }
+
   // One pair per slot (SameItem, DiffItem or, for F64, PairRef), swept in one
   // or (MULTI) several passes of 32R rows.
   __device__ static void run_item(const BatchView& b, const ClassLaunch& c, uint32_t item,
@@ -548,16 +571,22 @@ struct Forward {
     PairRef fr[2];
     load_refs(c, item, fr);
     const bool valid_y = P::kSlots == 2 && fr[1].read != kNoPair;
-    S res[2];
-    if (UNIFORM) {
+    double res[2] = {0.0, 0.0};
+    double amin[2] = {(double)kMinAcceptedF, (double)kMinAcceptedF};
+    if (kScaled) {
+      const uint32_t rows = passes * kWarp * R;
+      res[0] = scaled_result(b, fr[0].read, L[0], rows, P::sx(acc_m), P::sx(acc_i), &amin[0]);
+      if (valid_y)
+        res[1] = scaled_result(b, fr[1].read, L[1], rows, frozen_m, frozen_i, &amin[1]);
+    } else if (UNIFORM) {
       res[0] = uniform_gapm(b, fr[0].read) * P::sx(acc_m) + P::sx(acc_i);
       if (valid_y) res[1] = uniform_gapm(b, fr[1].read) * frozen_m + frozen_i;
     } else {
       res[0] = P::sx(acc_m) + P::sx(acc_i);
       res[1] = frozen_m + frozen_i;
     }
-    finish(b, c, fr[0], (double)res[0]);
-    if (valid_y) finish(b, c, fr[1], (double)res[1]);
+    finish(b, c, fr[0], res[0], amin[0]);
+    if (valid_y) finish(b, c, fr[1], res[1], amin[1]);
   }
 
   // A chain item: reads x and y against haplotypes hap_start .. +num_haps-1,
@@ -683,10 +712,11 @@ struct Forward {
       const double ratio = (double)(P::init_const() / (S)hl) / (double)init_s;
       const uint32_t hap = it.hap_start + gl;
       const uint32_t out = it.out_x + (uint32_t)gl * it.stride;
-      S res_x, res_y = 0;
+      double res_x, res_y = 0.0;
+      double amin_x = (double)kMinAcceptedF, amin_y = (double)kMinAcceptedF;
       if (kScaled) {
-        res_x = a.x + a.z;
-        res_y = a.y + a.w;
+        res_x = scaled_result(b, it.read_x, rx.len, GROUP * R, a.x, a.z, &amin_x);
+        if (has_y) res_y = scaled_result(b, it.read_y, ry.len, GROUP * R, a.y, a.w, &amin_y);
       } else if (UNIFORM) {
         res_x = uniform_gapm(b, it.read_x) * a.x + a.z;
         if (has_y) res_y = uniform_gapm(b, it.read_y) * a.y + a.w;
@@ -694,20 +724,30 @@ struct Forward {
         res_x = a.x + a.z;
         res_y = a.y + a.w;
       }
-      finish(b, c, PairRef{hap, it.read_x, out}, (double)res_x * ratio);
+      finish(b, c, PairRef{hap, it.read_x, out}, res_x * ratio, amin_x);
       if (has_y)
-        finish(b, c, PairRef{hap, it.read_y, out + (it.read_y - it.read_x)}, (double)res_y * ratio);
+        finish(b, c, PairRef{hap, it.read_y, out + (it.read_y - it.read_x)}, res_y * ratio,
+               amin_y);
     }
     __syncwarp();
   }
 
   // The final log10 of one pair from its scaled likelihood `raw` (an FP32
   // result, possibly rescaled in FP64, or an FP64 result).
-  // FP32: accepted at >= 1e-28 with an FP64 log10, else queued for FP64.
+  // FP32: accepted at >= accept_min (1e-28, the reference's bound, or the
+  // scaled form's bound) with an FP64 log10, else queued for FP64.
   __device__ static void finish(const BatchView& b, const ClassLaunch& c, const PairRef& ref,
-                                double raw) {
+                                double raw, double accept_min = (double)kMinAcceptedF) {
+    // A likelihood is finite and >= 0; anything else is an arithmetic fault,
+    // reported rather than passed on (it would fail the acceptance test and
+    // end up as a wrong FP64 value or -inf).
+    if (!(raw >= 0.0) || isinf(raw)) {
+      atomicOr(c.error_flags, kErrNonFinite);
+      b.out[ref.out] = CUDART_NAN;
+      return;
+    }
     if (P::kSlots == 2) {
-      if (raw >= (double)kMinAcceptedF) {
+      if (raw >= accept_min) {
         b.out[ref.out] = log10(raw) - kLog10InitF;
       } else {
         const uint32_t k = atomicAdd(c.rescue_count, 1u);
