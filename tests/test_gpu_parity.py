@@ -69,6 +69,26 @@ def test_assemble_regions_match_reference(engine):
     assert np.abs(got - oracle.batch_log10(b)).max() < TOL
 
 
+def test_fp64_rescue_only_where_fp32_falls_below_its_bound(engine):
+    """The FP64 pass must only see pairs whose FP32 likelihood is below the
+    acceptance bound: a wrong (NaN, zero) FP32 result would be rescued
+    silently and every value check would still pass.  The real chrY regions
+    all stay in FP32; on a synthetic batch the rescue count matches the
+    oracle's FP32 values below the bound (1e-28, or 1e-28/(mi*gapm) for the
+    scaled uniform-gap form) up to pairs within 1e-5 of it."""
+    b, _ = assemble_batch()
+    _, st = engine.batch(b, stats=True)
+    assert st["fp64_pairs"] == 0
+    b = workloads.make_workload("plain")
+    _, st = engine.batch(b, stats=True)
+    raw = oracle.batch_log10(b, oracle.FP32_RAW)
+    c = oracle.oracle_lib().oracle_ph2pr_f(45) * (1 - oracle.oracle_lib().oracle_ph2pr_f(10))
+    bound = 1e-28 / c          # every read of this workload has ins=del=45, gcp=10
+    below = int(np.sum(raw < bound))
+    near = int(np.sum(np.abs(raw / bound - 1) < 1e-5))
+    assert abs(st["fp64_pairs"] - below) <= near, (st["fp64_pairs"], below, near)
+
+
 def test_synthetic_n_bases_and_per_row_quals(engine):
     b, sched, intra = synthetic_batch()
     got = engine.batch(b)
