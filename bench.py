@@ -19,7 +19,8 @@ Reported (see the JSON keys):
   roofline   the FP32 forward kernels against the FP32 FMA peak measured on
              this GPU in this run (FMA-chain kernels, rodv_measure_peaks);
              12 algorithmic flops per cell (4 mul + 2 add for M, 2 mul + 1 add
-             for I and for D).
+             for I and for D); traffic is the DRAM bytes of those kernels per
+             step from an ncu capture of the full-size workload.
   plain_form the plain GPU form (one launch per pair) against the batched
              engine on the same sample.
   cpu_baseline  the reference's own schedule_pairhmm (oracle/_ref), threads
@@ -48,6 +49,19 @@ sys.path.insert(0, ROOT)
 METRIC = ("PairHMM GCUPS on 1 B200 (batched vs plain GPU form, % FP32 peak) vs host AVX; "
           "p99 ms")
 FLOPS_PER_CELL = 12
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "forward_kernels_dram_traffic_uneven_full.md")
+
+
+def step_traffic_bytes(workload, scale):
+    """DRAM bytes (read + write) of the FP32 kernels of one resident step, from the ncu
+    capture summarised in TRAFFIC_PROFILE; None for any other workload or size."""
+    if workload != "uneven" or scale != 1.0 or not os.path.exists(TRAFFIC_PROFILE):
+        return None
+    with open(TRAFFIC_PROFILE) as fh:
+        for ln in fh:
+            if ln.startswith("fp32_step_traffic_bytes:"):
+                return int(ln.split(":")[1])
+    return None
 
 
 def log(*a):
@@ -298,7 +312,11 @@ def run_engine(args, world, rank, local):
                     "ms_per_step": e2e_total / len(e2e_ms) * 1e3,
                     "max_abs_diff_vs_resident_run": same},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": step_traffic_bytes(args.workload, args.scale),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                           "of the FP32 kernels of one step (" +
+                                           os.path.relpath(TRAFFIC_PROFILE, ROOT) + ")",
                          "kernel": "forward_kernel<F32x2,...> (all FP32 classes of a step)",
                          "flops_per_cell": FLOPS_PER_CELL,
                          "peak_source": "FFMA-chain kernel measured in this run "
