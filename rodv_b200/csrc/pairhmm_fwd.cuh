@@ -181,8 +181,13 @@ __device__ __forceinline__ RowPriors<S> row_priors(uint32_t w, const PriorTables
 // Shared-memory shape of one warp's emission tables for R rows per lane
 // (kNumCodes codes; the separator code's entries are all 0).
 //   SAME layout (F64 always, F32x2 same-haplotype items): element (code, k)
-//     is one V; a 16-byte vector holds rows k, k+1 of the lane:
-//     vec index ((code * kNv + k/2) * 32 + lane).
+//     is one 8-byte V.  Per code, R/2 blocks of 16-byte vectors holding rows
+//     k, k+1 of each lane (vec index (code * kCodeVecs + k/2) * 32 + lane, in
+//     16-byte units), then, for odd R, one block of 8-byte entries holding the
+//     last row (byte offset code * kCodeBytes + (R/2) * 512 + lane * 8).  A
+//     step loads R/2 16-byte vectors and, for odd R, one 8-byte entry: R * 8
+//     bytes per lane, no padding row.  Both kinds of load are free of bank
+//     conflicts whatever code each lane reads (kCodeBytes is a multiple of 128).
 //   DIFF layout (F32x2 two-haplotype items): per slot, element (slot, code, k)
 //     is one float; a 16-byte vector holds rows k..k+3 of the lane:
 //     vec index (((slot * kNumCodes + code) * kNv + k/4) * 32 + lane).
@@ -191,9 +196,15 @@ struct TableShape {
   static constexpr bool kSameLayout = SAME || P::kSlots == 1;
   static constexpr int kRowsPerVec = kSameLayout ? 2 : 4;
   static constexpr int kRq = (R + kRowsPerVec - 1) / kRowsPerVec * kRowsPerVec;
-  static constexpr int kNv = kRq / kRowsPerVec;  // 16-byte loads per code (per slot)
+  static constexpr int kNv = kRq / kRowsPerVec;  // 16-byte loads per code (DIFF, per slot)
   static constexpr int kTables = kSameLayout ? 1 : 2;
-  static constexpr int kBytesPerWarp = kTables * kNumCodes * kNv * kWarp * 16;
+  // SAME layout: paired-row vectors and the odd last row per code
+  static constexpr int kPairVecs = R / 2;
+  static constexpr bool kOddRow = (R % 2) != 0;
+  static constexpr int kCodeBytes = kPairVecs * kWarp * 16 + (kOddRow ? kWarp * 8 : 0);
+  static constexpr int kBytesPerWarp =
+      kSameLayout ? kNumCodes * kCodeBytes : kTables * kNumCodes * kNv * kWarp * 16;
+  static_assert(!kSameLayout || kCodeBytes % 128 == 0, "code blocks must start on bank 0");
 };
 
 // Per-slot state of the pair being computed.
@@ -258,15 +269,20 @@ struct Forward {
     V mm[UNIFORM ? 1 : R], gapm[UNIFORM ? 1 : R], md[UNIFORM ? 1 : R];
     V mi[R], ii[R];
     V mmU, mdU, ddU;
+    V iiN;  // kScaled: ii of the next lane's first row (the row below this lane's last)
   };
 
   // Writes emission e of (slot, code, row k) into this lane's table.
   __device__ __forceinline__ static void put_emission(S* tab, int slot, int code, int k, int lane,
                                                       S e) {
     if (kSameHap) {
-      const int vec = (code * Shape::kNv + k / 2) * kWarp + lane;
-      // 16-byte vector = 2 rows of V; V = S[kSlots]
-      tab[vec * (16 / (int)sizeof(S)) + (k % 2) * P::kSlots + slot] = e;
+      static_assert(sizeof(V) == 8, "SAME layout entries are 8 bytes");
+      // V = S[kSlots]; a 16-byte vector holds 2 rows of V, an odd last row
+      // sits in the code's 8-byte block
+      const int byte = (k < 2 * Shape::kPairVecs)
+                           ? code * Shape::kCodeBytes + ((k / 2) * kWarp + lane) * 16 + (k % 2) * 8
+                           : code * Shape::kCodeBytes + Shape::kPairVecs * kWarp * 16 + lane * 8;
+      tab[byte / (int)sizeof(S) + slot] = e;
     } else {
       const int vec = ((slot * kNumCodes + code) * Shape::kNv + k / 4) * kWarp + lane;
       tab[vec * 4 + (k % 4)] = e;
@@ -356,6 +372,13 @@ struct Forward {
         p.md[UNIFORM ? 0 : k] = P::make(mdv[0], mdv[1]);
       }
     }
+    if (kScaled) {
+      const uint32_t row = first_row + R;
+      S iin[2];
+#pragma unroll
+      for (int s = 0; s < 2; ++s) iin[s] = row < L[s] ? u[s].ii : (row == L[s] ? u[s].mi : S(1));
+      p.iiN = P::make(iin[0], iin[1]);
+    }
   }
 
   // Emission values of this lane's rows for haplotype codes cx (slot x) and
@@ -363,13 +386,19 @@ struct Forward {
   __device__ __forceinline__ static void load_emission(const uint4* table, int lane, uint32_t cx,
                                                        uint32_t cy, V (&e)[R]) {
     if (kSameHap) {
-      const uint4* px = table + lane + cx * (Shape::kNv * kWarp);
+      const uint8_t* base = reinterpret_cast<const uint8_t*>(table) + cx * Shape::kCodeBytes;
+      const uint4* px = reinterpret_cast<const uint4*>(base) + lane;
 #pragma unroll
-      for (int v = 0; v < Shape::kNv; ++v) {
+      for (int v = 0; v < Shape::kPairVecs; ++v) {
         const uint4 raw = px[v * kWarp];
         const V* f = reinterpret_cast<const V*>(&raw);
-        if (2 * v < R) e[2 * v] = f[0];
-        if (2 * v + 1 < R) e[2 * v + 1] = f[1];
+        e[2 * v] = f[0];
+        e[2 * v + 1] = f[1];
+      }
+      if constexpr (Shape::kOddRow) {
+        const uint2 raw =
+            reinterpret_cast<const uint2*>(base + Shape::kPairVecs * kWarp * 16)[lane];
+        e[R - 1] = *reinterpret_cast<const V*>(&raw);
       }
     } else {
       S ex[Shape::kRq], ey[Shape::kRq];
@@ -431,6 +460,29 @@ struct Forward {
       um = M[k]; ui = I[k];
     }
     dg_m = up_m; dg_i = up_i; dg_d = up_d;
+  }
+
+  // cells() of the scaled form with the row above the lane's first row
+  // folded by the lane above (run_chain): t0 is the first row's M term
+  // (mm/c)*M~_d + I^_d + D^_d and i0 its I^, both computed by the lane above
+  // with the same operations cells() would apply here, so the results are
+  // bitwise the same while the lanes exchange two values a step instead of
+  // three.
+  __device__ __forceinline__ static void cells_scaled(const V (&e)[R], V t0, V i0, V (&M)[R],
+                                                      V (&I)[R], V (&D)[R], const Priors& p,
+                                                      V& t_last) {
+    V dm = P::zero(), di = P::zero(), dd = P::zero(), um = P::zero(), ui = P::zero();
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const V oM = M[k], oI = I[k], oD = D[k];
+      const V t = k == 0 ? t0 : P::fma(p.mmU, dm, P::add(di, dd));
+      M[k] = P::mul(t, e[k]);
+      if (k == R - 1) t_last = t;
+      I[k] = k == 0 ? i0 : P::fma(p.ii[k], ui, um);
+      D[k] = P::fma(p.ddU, oD, oM);
+      dm = oM; di = oI; dd = oD;
+      um = M[k]; ui = I[k];
+    }
   }
 
   // The two pairs of work item `item` (the second one's read is kNoPair when
@@ -670,6 +722,9 @@ struct Forward {
     for (int k = 0; k < R; ++k) M[k] = I[k] = D[k] = P::zero();
     V dg_m = P::zero(), dg_i = P::zero(), dg_d = P::zero();
     if (gl == 0) dg_d = init;
+    // scaled form: the first row's M term of the previous column (row 0 of
+    // the DP, D^ = init, for the group's first lane)
+    V dg_t = gl == 0 ? init : P::zero();
     const uint8_t* hx = b.hap_codes + co0 - gl;
     uint32_t hi = 0;                          // this lane's haplotype in the chain
     int nxt = (int)meta->sep[0] + gl;         // step at which this lane is at the next separator
@@ -683,15 +738,28 @@ struct Forward {
 
 #pragma unroll 2
     for (int s = 0; s < nsteps; ++s) {
-      V up_m = group_shfl_up(M[R - 1]);
-      V up_i = group_shfl_up(I[R - 1]);
-      V up_d = group_shfl_up(D[R - 1]);
-      if (gl == 0) {
-        up_m = P::zero(); up_i = P::zero(); up_d = init;
-      }
       V e[R], t_last;
-      load_emission(table, lane, hx[kGroups > 1 ? min(s, last_s) : s], 0u, e);
-      cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr, t_last);
+      if constexpr (kScaled) {
+        // the lane above hands over the M term (used one column later) and
+        // the I^ of this lane's first row
+        V in_t = group_shfl_up(P::fma(pr.mmU, M[R - 1], P::add(I[R - 1], D[R - 1])));
+        V in_i = group_shfl_up(P::fma(pr.iiN, I[R - 1], M[R - 1]));
+        if (gl == 0) {
+          in_t = init; in_i = P::zero();
+        }
+        load_emission(table, lane, hx[kGroups > 1 ? min(s, last_s) : s], 0u, e);
+        cells_scaled(e, dg_t, in_i, M, I, D, pr, t_last);
+        dg_t = in_t;
+      } else {
+        V up_m = group_shfl_up(M[R - 1]);
+        V up_i = group_shfl_up(I[R - 1]);
+        V up_d = group_shfl_up(D[R - 1]);
+        if (gl == 0) {
+          up_m = P::zero(); up_i = P::zero(); up_d = init;
+        }
+        load_emission(table, lane, hx[kGroups > 1 ? min(s, last_s) : s], 0u, e);
+        cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr, t_last);
+      }
       acc_m = P::fma(t_last, e[R - 1], acc_m);  // += M[R-1], one rounding
       acc_i = P::add(acc_i, I[R - 1]);
       if (s == nxt) {  // this lane just computed a separator column
