@@ -526,6 +526,66 @@ struct Forward {
     return len < rows ? (double)acc_i / mi : (double)acc_m / mi + (double)acc_i;
   }
 
+  // Early end of an FP32 multi-pass sweep.  Every alignment emits read row r
+  // from M or I at some column, and the transition and emission factors of
+  // the rest of a path are <= 1, so a pair's likelihood is at most
+  // sum_j (M + I)[r][j] for any row r.  After each pass but the last, the
+  // warp sums the boundary row (the pass's last row, kept for the next pass)
+  // and decides per slot whether that bound is below the FP32 acceptance
+  // bound, with a 1e-6 margin for the rounding of the remaining rows.  Such a
+  // pair is rejected at the end of the sweep whatever the remaining passes
+  // compute, so when both slots are decided the sweep stops and queues them
+  // for FP64 now: the same pairs reach FP64 and every result is unchanged.
+  // `row`: 0-based read row of the boundary; H: the slots' haplotype lengths.
+  __device__ static bool sweep_rejected(const BatchView& b, const ClassLaunch& c,
+                                        const BoundaryCell* buf, const uint32_t (&H)[2],
+                                        const uint32_t (&L)[2], uint32_t row, int lane,
+                                        uint32_t item) {
+    V sm = P::zero(), si = P::zero();
+    for (uint32_t col = 1 + (uint32_t)lane; col <= H[0]; col += kWarp) {
+      const BoundaryCell cell = buf[col];
+      const bool y_in = col <= H[1];
+      sm = P::add(sm, P::make(P::sx(cell.m), y_in ? P::sy(cell.m) : S(0)));
+      si = P::add(si, P::make(P::sx(cell.i), y_in ? P::sy(cell.i) : S(0)));
+    }
+    double sum_m[2] = {(double)P::sx(sm), (double)P::sy(sm)};
+    double sum_i[2] = {(double)P::sx(si), (double)P::sy(si)};
+#pragma unroll
+    for (int d = 16; d >= 1; d /= 2) {
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        sum_m[s] += __shfl_xor_sync(kFullMask, sum_m[s], d);
+        sum_i[s] += __shfl_xor_sync(kFullMask, sum_i[s], d);
+      }
+    }
+    PairRef refs[2];
+    load_refs(c, item, refs);
+    bool rejected = true;
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      if (s == 1 && refs[1].read == kNoPair) continue;
+      const uint32_t w = b.read_rows[b.reads[refs[s].read].row_off];
+      const double mi = (double)__ldg(Tables<S>::ph2pr(b.tab) + rw_ins(w));
+      const double gapm = 1.0 - (double)__ldg(Tables<S>::ph2pr(b.tab) + rw_gcp(w));
+      double bound, amin = (double)kMinAcceptedF;
+      if (kScaled) {
+        // M~ = mi * M and I^ = I; a pass-through row holds mi * (M_L + I_L) in I^
+        bound = row < L[s] ? sum_m[s] / mi + sum_i[s] : sum_i[s] / mi;
+        amin /= mi * gapm;
+      } else if (UNIFORM) {
+        bound = gapm * sum_m[s] + sum_i[s];  // M is kept divided by gapm
+      } else {
+        bound = sum_m[s] + sum_i[s];
+      }
+      rejected = rejected && bound >= 0.0 && bound < amin * 1e-6;
+    }
+    if (rejected && lane == 0) {
+      finish(b, c, refs[0], 0.0);
+      if (refs[1].read != kNoPair) finish(b, c, refs[1], 0.0);
+    }
+    return rejected;
+  }
+
   // One pair per slot (SameItem, DiffItem or, for F64, PairRef), swept in one
   // or (MULTI) several passes of 32R rows.
   __device__ static void run_item(const BatchView& b, const ClassLaunch& c, uint32_t item,
@@ -611,6 +671,11 @@ struct Forward {
         }
       }
       if (MULTI) __syncwarp();
+      if constexpr (MULTI && P::kSlots == 2) {
+        const uint32_t H[2] = {sl[0].H, sl[1].H};
+        if (!last && sweep_rejected(b, c, buf, H, L, (pass + 1) * (kWarp * R) - 1, lane, item))
+          return;
+      }
     }
 
     if (lane != kWarp - 1) return;

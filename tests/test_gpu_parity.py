@@ -89,6 +89,56 @@ def test_fp64_rescue_only_where_fp32_falls_below_its_bound(engine):
     assert abs(st["fp64_pairs"] - below) <= near, (st["fp64_pairs"], below, near)
 
 
+def test_multi_pass_sweeps_stop_only_for_pairs_fp32_rejects(engine):
+    """Long reads (several 256-row passes) that stay in FP32 mixed with long
+    reads whose likelihood falls below the FP32 bound after a few passes, with
+    uniform and per-row gap qualities.  A sweep may stop after a pass once
+    the boundary row's sum bounds the likelihood below the acceptance bound;
+    the pairs that reach FP64 must be exactly those whose full FP32 sweep is
+    below its bound, and every result must match the oracle."""
+    rng = np.random.default_rng(77)
+    regions, bounds = [], []
+    lib = oracle.oracle_lib()
+    for k in range(24):
+        hl = int(rng.integers(800, 1300))
+        hap = workloads._random_seq(rng, hl)
+        rl = int(rng.integers(600, 780))
+        start = int(rng.integers(0, hl - rl + 1))
+        fail = k % 2 == 0
+        rd = workloads._mutate(rng, hap[start:start + rl], 0.08 if fail else 0.001,
+                               0.01 if fail else 0.0)
+        n = len(rd)
+        q = workloads._quals(rng, n, 25, 40)
+        if k % 3 == 0:  # per-row gap qualities: the unscaled kernels
+            ins, dele, gcp = (workloads._quals(rng, n, 30, 45) for _ in range(3))
+            bounds.append(1e-28)
+        else:
+            ins = dele = np.full(n, 45, np.uint8)
+            gcp = np.full(n, 10, np.uint8)
+            bounds.append(1e-28 / (lib.oracle_ph2pr_f(45) * (1 - lib.oracle_ph2pr_f(10))))
+        reads = [rd]
+        if k % 4 == 1:  # a second read of the same haplotype: a same-haplotype item
+            rd2 = workloads._mutate(rng, hap[start:start + rl], 0.001, 0.0)
+            reads.append(rd2)
+            n2 = len(rd2)
+            ins2 = dele2 = np.full(n2, 45, np.uint8)
+            regions.append(([hap], reads, [q, workloads._quals(rng, n2, 25, 40)],
+                            [ins, ins2], [dele, dele2], [gcp, np.full(n2, 10, np.uint8)]))
+            bounds.append(bounds[-1] if k % 3 else 1e-28 / (
+                lib.oracle_ph2pr_f(45) * (1 - lib.oracle_ph2pr_f(10))))
+            continue
+        regions.append(([hap], reads, [q], [ins], [dele], [gcp]))
+    b = Batch.from_regions(regions)
+    got, st = engine.batch(b, stats=True)
+    ref = oracle.batch_log10(b)
+    assert np.abs(got - ref).max() < TOL
+    raw = oracle.batch_log10(b, oracle.FP32_RAW)
+    bounds = np.array(bounds)
+    below = int(np.sum(raw < bounds))
+    assert 0 < below < b.num_pairs
+    assert st["fp64_pairs"] == below, (st["fp64_pairs"], below)
+
+
 def test_synthetic_n_bases_and_per_row_quals(engine):
     b, sched, intra = synthetic_batch()
     got = engine.batch(b)
