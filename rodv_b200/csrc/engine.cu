@@ -464,10 +464,16 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   // ---- per region and class: reads, chain items, same items, leftovers ----
   // Single-pass reads of a region are sorted by (uniform gaps, length) and
   // paired neighbour by neighbour; a pair's class is that of its longer read
-  // (uniform only if both are), an odd last read forms a one-read chain.
-  // Each pair takes ceil(haps / chain_haps[class]) chain items.  Multi-pass reads
-  // keep their own class: same-haplotype items per haplotype, leftovers in
-  // two-haplotype items.
+  // (uniform only if both are).  Each pair takes ceil(haps / chain_haps[class])
+  // chain items.  An odd last read is a leftover: its pairs (one per
+  // haplotype) go into two-haplotype items with other regions' leftover
+  // pairs of its class, so that both halves of the f32x2 lanes work (a
+  // one-read chain leaves one half idle; a batch of one-read regions ran at
+  // half the FP32 rate).  Whether a read is a leftover depends on its region
+  // only, and a pair's arithmetic in a two-haplotype item does not depend on
+  // its partner, so results do not depend on the rest of the batch.
+  // Multi-pass reads keep their own class: same-haplotype items per
+  // haplotype, leftovers in two-haplotype items.
   const uint32_t K = kNumClasses;
   auto sorted_single = [&](const rodv_region& rg, std::vector<uint32_t>& out_reads) {
     out_reads.clear();
@@ -493,6 +499,8 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   std::vector<uint32_t> hmax(G, 0);
   // multi-pass leftovers: the last read of each multi-pass class in the region
   std::vector<uint32_t> left_read((size_t)G * 2, kNoPair);
+  // single-pass leftover: the odd last read of the region's sorted single-pass reads
+  std::vector<uint32_t> single_read(G, kNoPair);
   parallel_for(G, 64, [&](size_t lo, size_t hi) {
     std::vector<uint32_t> sr;
     for (size_t g = lo; g < hi; ++g) {
@@ -514,8 +522,11 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       for (size_t k = 0; k < sr.size(); k += 2) {
         const bool two = k + 1 < sr.size();
         const int c = two ? pair_class(sr[k], sr[k + 1]) : read_class[sr[k]];
-        rpairs[g * K + c] += 1;
         cpairs[g * K + c] += (uint64_t)rg.num_haps * (two ? 2 : 1);
+        if (two)
+          rpairs[g * K + c] += 1;
+        else
+          single_read[g] = sr[k];
       }
     }
   });
@@ -571,6 +582,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       } else {
         same_tot[c] += chains[(size_t)g * K + c];
         cap_tot[c] += cpairs[(size_t)g * K + c];
+        if (single_read[g] != kNoPair && read_class[single_read[g]] == c) left_tot[c] += H;
       }
     }
   }
@@ -590,9 +602,11 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
     // forced, every pair whose read is of class c)
     plan.pairs[c] = (uint32_t)(fp64 ? list_tot[c] : cap_tot[c]);
     plan.same_items[c] = fp64 ? 0u : (uint32_t)same_tot[c];
-    uint64_t diff = 0;
-    if (class_multi(c))
+    uint64_t diff = (left_tot[c] + 1) / 2;  // single-pass leftovers pair freely
+    if (class_multi(c)) {
+      diff = 0;
       for (uint64_t n : left_by_passes[c - kSinglePassClasses]) diff += (n + 1) / 2;
+    }
     plan.diff_items[c] = fp64 ? 0u : (uint32_t)diff;
   }
   for (uint32_t g = 0; g < G; ++g) {
@@ -729,15 +743,20 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
         sorted_single(rg, sr);
         uint64_t next[kNumClasses];
         for (int c = 0; c < kNumClasses; ++c) next[c] = same_off[g * K + c];
-        for (size_t k = 0; k < sr.size(); k += 2) {
-          const bool two = k + 1 < sr.size();
-          const int c = two ? pair_class(sr[k], sr[k + 1]) : read_class[sr[k]];
+        for (size_t k = 0; k + 1 < sr.size(); k += 2) {
+          const int c = pair_class(sr[k], sr[k + 1]);
           ChainItem* ci = reinterpret_cast<ChainItem*>(s + plan.off_same[c]);
           const uint32_t cap = plan.chain_haps[c];
           for (uint32_t h0 = 0; h0 < rg.num_haps; h0 += cap)
             ci[next[c]++] = ChainItem{rg.hap_start + h0, std::min(cap, rg.num_haps - h0), sr[k],
-                                      two ? sr[k + 1] : kNoPair, out_of(h0, sr[k]), N, hmax[g],
-                                      0};
+                                      sr[k + 1], out_of(h0, sr[k]), N, hmax[g], 0};
+        }
+        if (single_read[g] != kNoPair) {
+          const uint32_t rr = single_read[g];
+          const int c = read_class[rr];
+          PairRef* lf = leftovers[c].data() + left_off[g * K + c];
+          for (uint32_t h = 0; h < rg.num_haps; ++h)
+            lf[h] = PairRef{rg.hap_start + h, rr, out_of(h, rr)};
         }
       }
       for (auto& v : byclass) v.clear();
@@ -763,9 +782,10 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
     }
   });
   if (!fp64) {
-    // leftovers: grouped by pass count, sorted by haplotype length within a
-    // group, paired longest-first within the group
-    for (int c = kSinglePassClasses; c < kNumClasses; ++c) {
+    // leftovers: grouped by pass count (single-pass classes: one group),
+    // sorted by haplotype length within a group (slot x takes the longer
+    // haplotype), paired longest-first within the group
+    for (int c = 0; c < kNumClasses; ++c) {
       std::vector<PairRef>& lv = leftovers[c];
       std::stable_sort(lv.begin(), lv.end(), [&](const PairRef& x, const PairRef& y) {
         const uint32_t px = passes_of(x.read), py = passes_of(y.read);
@@ -962,7 +982,11 @@ rodv_status Engine::finish_lane(HostLane& l, double* out, rodv_stats* st) {
   if (counts[kCtrError] != 0)
     return fail(RODV_ERR_DEVICE_CHECK,
                 "kernel reported error flags " + std::to_string(counts[kCtrError]));
-  std::memcpy(out + l.out_off, h, p.num_pairs * 8);
+  // results into the caller's (pageable) buffer, 128K pairs per task: the
+  // last range's copy is on the call's critical path
+  parallel_for(p.num_pairs, 1u << 17, [&](size_t lo, size_t hi) {
+    std::memcpy(out + l.out_off + lo, h + lo * 8, (hi - lo) * 8);
+  });
   if (st) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, l.ev[0], l.ev[2]);
@@ -1112,7 +1136,9 @@ rodv_status Engine::run_host_single(const rodv_batch& b, double* out, rodv_stats
   if (counts[kCtrError] != 0)
     return fail(RODV_ERR_DEVICE_CHECK,
                 "kernel reported error flags " + std::to_string(counts[kCtrError]));
-  std::memcpy(out, hs, plan.num_pairs * 8);
+  parallel_for(plan.num_pairs, 1u << 17, [&](size_t lo, size_t hi) {
+    std::memcpy(out + lo, hs + lo * 8, (hi - lo) * 8);
+  });
   if (st) {
     fill_stats(st, plan, counts);
     float ms = 0.f;

@@ -67,15 +67,10 @@ KernelInfo info_for(Precision prec, bool uniform, bool same, int variant) {
   if (same)
     return uniform ? variant_info<F32x2, R, true, MU, true>(variant)
                    : variant_info<F32x2, R, false, MU, true>(variant);
-  // Two-haplotype items exist for multi-pass reads only (single-pass reads
-  // of a region all go into chain items).
-  if constexpr (MU) {
-    return uniform ? variant_info<F32x2, R, true, MU, false>(0)
-                   : variant_info<F32x2, R, false, MU, false>(0);
-  } else {
-    (void)uniform;
-    return KernelInfo{};
-  }
+  // Two-haplotype items: multi-pass leftovers, and the odd single-pass read
+  // of a region against each of its haplotypes.
+  return uniform ? variant_info<F32x2, R, true, MU, false>(0)
+                 : variant_info<F32x2, R, false, MU, false>(0);
 }
 
 }  // namespace rodv

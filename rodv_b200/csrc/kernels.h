@@ -33,7 +33,8 @@ constexpr int kMaxGroupedRows = 4;  // classes with R <= 4 have the grouped vari
 // Forward kernel for one work class.  rows_per_lane in 1..8; multi kernels
 // always use 8 rows per lane.  same: FP32 items whose reads share the
 // haplotypes -- ChainItem for single-pass classes, SameItem for multi-pass
-// ones; !same: DiffItem (multi-pass only; fn is null for a single-pass class).
+// ones; !same: DiffItem (multi-pass leftovers; in a single-pass class, the
+// pairs of each region's odd read).
 // FP64 kernels take PairRef lists.  variant < forward_kernel_variants(...)
 // selects the variant of same-haplotype FP32 kernels.
 KernelInfo forward_kernel_info(Precision prec, int rows_per_lane, bool uniform, bool multi,

@@ -139,6 +139,27 @@ def test_multi_pass_sweeps_stop_only_for_pairs_fp32_rejects(engine):
     assert st["fp64_pairs"] == below, (st["fp64_pairs"], below)
 
 
+def test_odd_reads_pair_across_regions_without_changing_results(engine):
+    """The odd single-pass read of a region (every read of a one-read region)
+    is computed in two-haplotype items with other regions' odd reads.  Its
+    results must match the oracle and be bitwise the same whether its region
+    runs alone (no partner) or in a batch (a partner from another region)."""
+    rng = np.random.default_rng(31)
+    regions = []
+    for k in range(40):
+        nh = int(rng.integers(1, 6))
+        nr = 1 if k % 2 == 0 else 3
+        regions.append(workloads.random_region(rng, nh, nr, hap_len=(40, 400),
+                                               read_len=(10, 250), vary_gap_quals=k % 4 == 1))
+    b = Batch.from_regions(regions)
+    got = engine.batch(b)
+    assert np.abs(got - oracle.batch_log10(b)).max() < TOL
+    off = b.out_offsets()
+    for g in range(0, len(regions), 3):
+        alone = engine.batch(b.subset([g]))
+        assert np.array_equal(alone, got[int(off[g]):int(off[g + 1])]), g
+
+
 def test_synthetic_n_bases_and_per_row_quals(engine):
     b, sched, intra = synthetic_batch()
     got = engine.batch(b)
