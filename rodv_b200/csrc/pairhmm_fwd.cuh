@@ -801,9 +801,15 @@ struct Forward {
     // code index stays clamped there so it reads no byte past its chain.
     const int last_s = (int)ncols + gl;
 
+    // the haplotype code of the next step is loaded one step ahead (the
+    // emission loads wait on it); at most one byte past the last step's,
+    // inside the code array's tail padding
+    uint32_t code_next = hx[0];
 #pragma unroll 2
     for (int s = 0; s < nsteps; ++s) {
       V e[R], t_last;
+      const uint32_t code = code_next;
+      code_next = hx[kGroups > 1 ? min(s + 1, last_s) : s + 1];
       if constexpr (kScaled) {
         // the lane above hands over the M term (used one column later) and
         // the I^ of this lane's first row
@@ -812,7 +818,7 @@ struct Forward {
         if (gl == 0) {
           in_t = init; in_i = P::zero();
         }
-        load_emission(table, lane, hx[kGroups > 1 ? min(s, last_s) : s], 0u, e);
+        load_emission(table, lane, code, 0u, e);
         cells_scaled(e, dg_t, in_i, M, I, D, pr, t_last);
         dg_t = in_t;
       } else {
@@ -822,7 +828,7 @@ struct Forward {
         if (gl == 0) {
           up_m = P::zero(); up_i = P::zero(); up_d = init;
         }
-        load_emission(table, lane, hx[kGroups > 1 ? min(s, last_s) : s], 0u, e);
+        load_emission(table, lane, code, 0u, e);
         cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr, t_last);
       }
       acc_m = P::fma(t_last, e[R - 1], acc_m);  // += M[R-1], one rounding
