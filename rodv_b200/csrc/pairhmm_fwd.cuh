@@ -238,11 +238,15 @@ struct Forward {
   static constexpr int kGroups = kWarp / GROUP;       // chain items per warp
   static constexpr int kGroupHaps = kChainHaps / kGroups;  // haplotypes per chain item
   static_assert(GROUP == 32 || kChain, "lane groups are for chain kernels only");
-  // FP32 kernels of the uniform-gap classes use the scaled 5-operation form
-  // (reads of these classes have equal insertion and deletion quality).  The
-  // FP64 kernels keep the unscaled form: they have no fallback, and the scaled
-  // form would lose precision just above the reference's FP64 underflow limit.
-  static constexpr bool kScaled = UNIFORM && P::kSlots == 2;
+  // Kernels of the uniform-gap classes use the scaled 5-operation form
+  // (reads of these classes have equal insertion and deletion quality), FP64
+  // ones too.  The form keeps I and D at the reference's magnitude and M
+  // mi times smaller (mi*gapm >= 1e-6 in these classes), so it reaches the
+  // FP64 denormal range only for pairs whose likelihood is within that factor
+  // of the 2^1020 scaling's underflow limit (log10 about -615, below which
+  // the reference returns -inf); there M keeps at least 32 of its 52
+  // mantissa bits (37 at ins = del = 45, gcp = 10), 1e-10 relative or better.
+  static constexpr bool kScaled = UNIFORM;
   static constexpr int kWarpsPerBlock = 4;
   static constexpr int kSmemPerWarp =
       Shape::kBytesPerWarp + (kChain ? kGroups * (int)sizeof(ChainMeta) : 0);
