@@ -304,7 +304,15 @@ __global__ void na_pairs_kernel(NaArgs a) {
   }
 }
 
-// Per-device set-up: the scratch array's device address, tables copied in.
+// Dynamic shared memory per block of the two kernels.
+constexpr int kSmemF32 = Forward<F32x2, kMaxRowsPerLane, false, true, false, 1>::kWarpsPerBlock *
+                         Forward<F32x2, kMaxRowsPerLane, false, true, false, 1>::kSmemPerWarp;
+constexpr int kSmemF64 = Forward<F64, kMaxRowsPerLane, false, true, false, 1>::kWarpsPerBlock *
+                         Forward<F64, kMaxRowsPerLane, false, true, false, 1>::kSmemPerWarp;
+static_assert(kSmemF32 <= 227 * 1024 && kSmemF64 <= 227 * 1024, "tables too large");
+
+// Per-device set-up: the scratch array's device address, tables copied in,
+// the kernels' shared-memory limit raised.
 struct DeviceSlot {
   std::once_flag once;
   unsigned char* ptr = nullptr;
@@ -328,6 +336,14 @@ cudaError_t setup_device(int dev, unsigned char** out) {
         e = cudaMemcpy(s + kOffPh2prD, t.ph2pr_d.data(), 128 * 8, cudaMemcpyHostToDevice);
       if (e == cudaSuccess)
         e = cudaMemcpy(s + kOffMmD, t.mm_d.data(), kMmTableSize * 8, cudaMemcpyHostToDevice);
+      // the two kernels' shared memory (tables and boundary ring) may exceed
+      // the default 48 KB per block
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(&forward_kernel<F32x2, kMaxRowsPerLane, false, true, false, 1>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemF32);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(&forward_kernel<F64, kMaxRowsPerLane, false, true, false, 1>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemF64);
     }
     slot.err = e;
     slot.ptr = (e == cudaSuccess) ? static_cast<unsigned char*>(p) : nullptr;
@@ -393,9 +409,6 @@ extern "C" rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32
 
   using F32 = Forward<F32x2, kMaxRowsPerLane, false, true, false, 1>;
   using D64 = Forward<F64, kMaxRowsPerLane, false, true, false, 1>;
-  // launched without the dynamic shared-memory opt-in
-  static_assert(F32::kWarpsPerBlock * F32::kSmemPerWarp <= 48 * 1024, "F32 table too large");
-  static_assert(D64::kWarpsPerBlock * D64::kSmemPerWarp <= 48 * 1024, "F64 table too large");
   ClassLaunch c32{};
   c32.work = s + kOffItems;
   c32.work_count = cnt + kCItems;

@@ -92,6 +92,18 @@ __device__ __forceinline__ float2 f2_value(unsigned long long r) {
   return v;
 }
 
+// cp.async of 8 bytes global -> shared (through L1), and its group controls.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 struct F32x2 {
   using V = float2;
   using S = float;
@@ -248,8 +260,12 @@ struct Forward {
   // mantissa bits (37 at ins = del = 45, gcp = 10), 1e-10 relative or better.
   static constexpr bool kScaled = UNIFORM;
   static constexpr int kWarpsPerBlock = 4;
+  // Multi-pass kernels also keep a ring of 2 x 32 boundary cells per warp
+  // (the next 32 columns of the previous pass's last row, see run_item).
+  static constexpr int kRingCells = 2 * kWarp;
   static constexpr int kSmemPerWarp =
-      Shape::kBytesPerWarp + (kChain ? kGroups * (int)sizeof(ChainMeta) : 0);
+      Shape::kBytesPerWarp + (kChain ? kGroups * (int)sizeof(ChainMeta) : 0) +
+      (MULTI ? kRingCells * 3 * (int)sizeof(V) : 0);
 
   // Shuffles within a lane group (the row above comes from the previous lane
   // of the same group).
@@ -624,6 +640,25 @@ struct Forward {
 
     BoundaryCell* buf = nullptr;
     if (MULTI) buf = reinterpret_cast<BoundaryCell*>(c.scratch) + (size_t)gwarp * c.scratch_cols;
+    // Lane 0 of a pass after the first takes the row above from the previous
+    // pass's boundary row in scratch, one cell per step.  Read from global
+    // memory at each step, that load's latency sat on every step's critical
+    // path; instead the warp copies the cells of the next 32 steps into a
+    // shared-memory ring with cp.async (one cell per lane, coalesced) while it
+    // computes the current 32, and lane 0 reads the ring.  Copies stop at the
+    // warp's scratch_cols (cells past the last step's are never read).
+    BoundaryCell* ring = reinterpret_cast<BoundaryCell*>(table + Shape::kBytesPerWarp / 16);
+    auto fetch_chunk = [&](int chunk) {  // cells of steps [32 chunk, 32 chunk + 32)
+      const uint32_t idx = (uint32_t)chunk * kWarp + 1u + (uint32_t)lane;
+      if (idx < c.scratch_cols) {
+        BoundaryCell* dst = ring + (chunk & 1) * kWarp + lane;
+        const BoundaryCell* src = buf + idx;
+        cp_async8(&dst->m, &src->m);
+        cp_async8(&dst->i, &src->i);
+        cp_async8(&dst->d, &src->d);
+      }
+      cp_async_commit();
+    };
 
     V acc_m = P::zero(), acc_i = P::zero();
     S frozen_m = 0, frozen_i = 0;
@@ -640,15 +675,22 @@ struct Forward {
       if (lane == 0 && pass == 0) dg_d = init;
       const uint8_t* hx = sl[0].hap - lane;
       const uint8_t* hy = sl[1].hap - lane;
+      const bool from_ring = MULTI && pass > 0;
+      if (from_ring) fetch_chunk(0);
 
 #pragma unroll 2
       for (int s = 0; s < nsteps; ++s) {
+        if (from_ring && (s & (kWarp - 1)) == 0) {
+          cp_async_wait_all();  // this chunk's cells
+          __syncwarp();
+          fetch_chunk(s / kWarp + 1);
+        }
         V up_m = P::shfl_up(M[R - 1]);
         V up_i = P::shfl_up(I[R - 1]);
         V up_d = P::shfl_up(D[R - 1]);
         if (lane == 0) {
-          if (MULTI && pass > 0) {
-            const BoundaryCell cell = buf[s + 1];
+          if (from_ring) {
+            const BoundaryCell cell = ring[((s / kWarp) & 1) * kWarp + (s & (kWarp - 1))];
             up_m = cell.m; up_i = cell.i; up_d = cell.d;
           } else {
             up_m = P::zero(); up_i = P::zero(); up_d = init;
@@ -674,7 +716,10 @@ struct Forward {
           }
         }
       }
-      if (MULTI) __syncwarp();
+      if (MULTI) {
+        cp_async_wait_all();  // the prefetch past the last step lands before the ring is reused
+        __syncwarp();
+      }
       if constexpr (MULTI && P::kSlots == 2) {
         const uint32_t H[2] = {sl[0].H, sl[1].H};
         if (!last && sweep_rejected(b, c, buf, H, L, (pass + 1) * (kWarp * R) - 1, lane, item))
