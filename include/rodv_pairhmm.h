@@ -182,8 +182,8 @@ rodv_status rodv_measure_peaks(rodv_engine* engine, double* fp32_gflops, double*
  * Same results as rodv_pairhmm_batch (every pair through the per-row-prior
  * multi-pass kernels).  Returns after the work on `stream` has finished.
  * The first call on a device sets that device up (obtains the scratch
- * address, copies the prior tables) and synchronises it: make it before any
- * stream capture.  All calls in a process share the scratch array: calls
+ * address, copies the prior tables, raises its two kernels' shared-memory
+ * limit per block) and synchronises it: make it before any stream capture.  All calls in a process share the scratch array: calls
  * that overlap on the GPU race and must be serialised by the caller.
  * Sizes beyond the limits below return RODV_ERR_TOO_LONG; on any error the
  * output contents are unspecified. */

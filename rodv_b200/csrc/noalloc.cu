@@ -27,9 +27,11 @@
 //
 // Set-up.  Host code cannot use the array's name as a device address: in host
 // code it names a host-side stand-in.  The first call on each device (with
-// that device current) obtains the real address with cudaGetSymbolAddress and
-// copies the prior tables into the array; that first call synchronises the
-// device and must come before any stream capture.
+// that device current) obtains the real address with cudaGetSymbolAddress,
+// copies the prior tables into the array and raises the two forward kernels'
+// dynamic shared-memory limit (their tables and boundary ring take more than
+// the default 48 KB per block; a function attribute, not an allocation); that
+// first call synchronises the device and must come before any stream capture.
 //
 // The array is shared by every call in the process on that device and keeps
 // the last call's contents; each call clears the counters and pads it depends
