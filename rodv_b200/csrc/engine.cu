@@ -919,7 +919,9 @@ static void fill_stats(rodv_stats* st, const PackedPlan& plan, const uint32_t* c
 // kChunkCells cells.  Results do not depend on the cut (a pair's arithmetic
 // depends on its own region only).  Measured on the 10,000-region uneven
 // batch (5.1e11 cells): 3e10-cell ranges 171 ms, 6e10 158 ms, 1.2e11 150 ms
-// per call, against 139 ms of resident compute.
+// per call, against 139 ms of resident compute (with later kernels: 146-148
+// ms against 133).  Running every range's kernels on one stream was slower
+// (159 ms): concurrent ranges fill each other's per-class tails.
 constexpr double kChunkCells = 1.2e11;
 constexpr double kFirstChunkCells = 4e9;
 constexpr double kMinChunkedCells = 2e10;
