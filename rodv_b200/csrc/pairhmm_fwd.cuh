@@ -677,9 +677,16 @@ struct Forward {
       const uint8_t* hy = sl[1].hap - lane;
       const bool from_ring = MULTI && pass > 0;
       if (from_ring) fetch_chunk(0);
+      // codes of the next step loaded one step ahead (the emission loads wait
+      // on them); the last step's read lands one byte further into the code
+      // array's tail padding
+      uint32_t cx_next = hx[0], cy_next = kSameHap ? 0u : (uint32_t)hy[0];
 
 #pragma unroll 2
       for (int s = 0; s < nsteps; ++s) {
+        const uint32_t cx = cx_next, cy = cy_next;
+        cx_next = hx[s + 1];
+        if (!kSameHap) cy_next = hy[s + 1];
         if (from_ring && (s & (kWarp - 1)) == 0) {
           cp_async_wait_all();  // this chunk's cells
           __syncwarp();
@@ -697,7 +704,7 @@ struct Forward {
           }
         }
         V e[R], t_last;
-        load_emission(table, lane, hx[s], kSameHap ? 0u : (uint32_t)hy[s], e);
+        load_emission(table, lane, cx, cy, e);
         cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr, t_last);
         if (MULTI && !last && lane == kWarp - 1) {
           const int col = s - (kWarp - 1) + 1;
