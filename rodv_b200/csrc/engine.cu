@@ -233,6 +233,12 @@ Engine::~Engine() {
     cudaStreamSynchronize(stream_);
     for (auto& e : ev_) cudaEventDestroy(e);
     cudaStreamDestroy(stream_);
+    for (int c = 0; c < kNumClasses; ++c) {
+      if (side_[c]) cudaStreamSynchronize(side_[c]);
+      if (side_[c]) cudaStreamDestroy(side_[c]);
+      if (join_ev_[c]) cudaEventDestroy(join_ev_[c]);
+    }
+    if (fork_ev_) cudaEventDestroy(fork_ev_);
     for (HostLane& l : lanes_) {
       if (l.stream) cudaStreamSynchronize(l.stream);
       for (cudaEvent_t e : l.ev)
@@ -279,6 +285,11 @@ rodv_status Engine::init() {
   RODV_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   for (auto& e : ev_) RODV_CUDA(cudaEventCreate(&e));
   ready_ = true;  // the destructor releases what was created
+  RODV_CUDA(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
+  for (int c = 0; c < kNumClasses; ++c) {
+    RODV_CUDA(cudaStreamCreateWithFlags(&side_[c], cudaStreamNonBlocking));
+    RODV_CUDA(cudaEventCreateWithFlags(&join_ev_[c], cudaEventDisableTiming));
+  }
   for (HostLane& l : lanes_) {
     RODV_CUDA(cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking));
     for (auto& e : l.ev) RODV_CUDA(cudaEventCreate(&e));
@@ -848,9 +859,33 @@ rodv_status Engine::launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, in
 }
 
 rodv_status Engine::launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stats* st,
-                               cudaStream_t stream, cudaEvent_t* ev, int parts) {
+                               cudaStream_t stream, cudaEvent_t* ev, int parts, bool fan_out) {
   ArenaView a = arena_view(plan, dbase, tab_);
   uint32_t launches = 0;
+  // fan-out: the first launch of class c waits on the fork point on side_[c];
+  // join() brings every used side stream back into `stream`
+  bool forked[kNumClasses] = {};
+  auto lane = [&](int c) -> cudaStream_t {
+    if (!fan_out) return stream;
+    if (!forked[c]) {
+      if (cudaStreamWaitEvent(side_[c], fork_ev_, 0) != cudaSuccess) return nullptr;
+      forked[c] = true;
+    }
+    return side_[c];
+  };
+  auto fork = [&]() -> cudaError_t {
+    for (bool& f : forked) f = false;
+    return fan_out ? cudaEventRecord(fork_ev_, stream) : cudaSuccess;
+  };
+  auto join = [&]() -> cudaError_t {
+    for (int c = 0; c < kNumClasses && fan_out; ++c) {
+      if (!forked[c]) continue;
+      cudaError_t e = cudaEventRecord(join_ev_[c], side_[c]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, join_ev_[c], 0);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  };
   if (parts & 1) {
     RODV_CUDA(cudaMemsetAsync(a.counts, 0, kCountWords * 4, stream));
     if (plan.fp64)  // every pair goes to the FP64 kernels: the uploaded lists are full
@@ -859,16 +894,21 @@ rodv_status Engine::launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stat
   }
   if (ev) RODV_CUDA(cudaEventRecord(ev[0], stream));
   if (!plan.fp64 && (parts & 1)) {
+    RODV_CUDA(fork());
     for (int c = 0; c < kNumClasses; ++c) {
       for (int same = 1; same >= 0; --same) {
         if (!(same ? plan.same_items[c] : plan.diff_items[c])) continue;
-        rodv_status s = launch_fp32_class(plan, dbase, c, same != 0, plan.variant[c], 0, stream);
+        const cudaStream_t ls = lane(c);
+        if (!ls) return cuda_fail(cudaErrorUnknown, "class stream fork");
+        rodv_status s = launch_fp32_class(plan, dbase, c, same != 0, plan.variant[c], 0, ls);
         if (s != RODV_OK) return s;
         ++launches;
       }
     }
+    RODV_CUDA(join());
   }
   if (ev) RODV_CUDA(cudaEventRecord(ev[1], stream));
+  if (parts & 2) RODV_CUDA(fork());
   for (int c = 0; c < kNumClasses && (parts & 2); ++c) {
     if (!plan.pairs[c]) continue;
     const KernelInfo k =
@@ -884,9 +924,12 @@ rodv_status Engine::launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stat
     const int need = (int)((plan.pairs[c] + k.warps_per_block - 1) / k.warps_per_block);
     const int blocks = std::max(1, std::min(persistent_blocks(k), need));
     void* args[] = {&a.view, &cl};
-    RODV_CUDA(cudaLaunchKernel(k.fn, dim3(blocks), dim3(k.threads), args, k.smem_bytes, stream));
+    const cudaStream_t ls = lane(c);
+    if (!ls) return cuda_fail(cudaErrorUnknown, "class stream fork");
+    RODV_CUDA(cudaLaunchKernel(k.fn, dim3(blocks), dim3(k.threads), args, k.smem_bytes, ls));
     ++launches;
   }
+  if (parts & 2) RODV_CUDA(join());
   if (ev) RODV_CUDA(cudaEventRecord(ev[2], stream));
   if (st) st->kernel_launches += launches;
   return RODV_OK;
@@ -1186,11 +1229,14 @@ rodv_status Engine::run_device(rodv_device_batch* db, rodv_stats* st) {
   if (!db->graph[0]) {
     // Capture once, as two graphs (FP32 part: counter reset and the FP32 class
     // launches; FP64 part: the rescue launches) so that an event between them
-    // times the FP32 pass; later runs are two graph launches.
+    // times the FP32 pass; later runs are two graph launches.  Within each
+    // graph the classes are parallel branches (independent items, counters
+    // and rescue lists), so one class's kernel starts in another's tail.
     for (int part = 0; part < 2; ++part) {
       rodv_stats cap{};
       RODV_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
-      rodv_status s = launch_all(db->plan, d, &cap, stream_, nullptr, part == 0 ? 1 : 2);
+      rodv_status s =
+          launch_all(db->plan, d, &cap, stream_, nullptr, part == 0 ? 1 : 2, /*fan_out=*/true);
       cudaGraph_t g = nullptr;
       const cudaError_t ce = cudaStreamEndCapture(stream_, &g);
       if (s != RODV_OK) {

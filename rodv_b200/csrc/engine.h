@@ -135,9 +135,13 @@ class Engine {
   rodv_status pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64);
   // parts: 1 = counter reset and FP32 launches, 2 = FP64 launches.  ev: null,
   // or three events recorded before the FP32 launches, between the two parts
-  // and after the FP64 launches.
+  // and after the FP64 launches.  fan_out: each class's launches go to its own
+  // side stream (forked from and joined back into `stream`), so that class
+  // kernels fill each other's tails; for the captured resident path, whose
+  // engine-owned side streams no other caller uses at the same time.
   rodv_status launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stats* st,
-                         cudaStream_t stream, cudaEvent_t* ev, int parts);
+                         cudaStream_t stream, cudaEvent_t* ev, int parts,
+                         bool fan_out = false);
   rodv_status launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, int cls, bool same,
                                 int variant, int blocks_cap, cudaStream_t stream);
   rodv_status check_errors(const PackedPlan& plan, uint8_t* dbase);
@@ -158,6 +162,8 @@ class Engine {
   std::string device_name_;
   cudaStream_t stream_ = nullptr;
   cudaEvent_t ev_[4] = {};
+  cudaStream_t side_[kNumClasses] = {};  // launch_all fan-out, one per class
+  cudaEvent_t fork_ev_ = nullptr, join_ev_[kNumClasses] = {};
   DeviceMem tables_;
   PriorTables tab_{};
   int variant_[kNumClasses] = {};          // tuned occupancy variant per class
