@@ -135,6 +135,17 @@ rodv_status rodv_pairhmm_batch(rodv_engine* engine, const rodv_batch* batch, int
 /* Number of results of a batch (sum of num_haps*num_reads). */
 uint64_t rodv_batch_num_pairs(const rodv_batch* batch);
 
+/* Checks a batch on the host, without a device, by the rules the compute
+ * calls apply: at least one region; every region with haplotypes and reads
+ * and indexing inside the arrays; no empty sequence; lengths within the
+ * limits above; fewer than 2^32 pairs; bases A, C, G, T or N.  Returns
+ * RODV_OK or the status a compute call would return for the batch; msg (may
+ * be null) receives a description, at most msg_len bytes including the
+ * terminating zero.  No counterpart in the reference: schedule_pairhmm checks
+ * only for M == 0 or N == 0 (pairhmm_schedule.cpp:130-132) and reads other
+ * invalid input out of bounds. */
+rodv_status rodv_batch_validate(const rodv_batch* batch, char* msg, size_t msg_len);
+
 /* One pair (computeLikelihoodsAVX512(tc, use_double), pairhmm_api.h:17-20):
  * FP32 with FP64 rescue below 1e-28, or FP64 when use_double != 0. */
 rodv_status rodv_pairhmm_pair(rodv_engine* engine, const uint8_t* hap, uint32_t hap_len,

@@ -27,7 +27,7 @@ from ._lib import RodvError
 from .batch import Batch
 
 __all__ = ["Engine", "DeviceBatch", "Service", "Batch", "RodvError", "schedule_pairhmm",
-           "compute_likelihoods", "TestCase", "default_engine"]
+           "compute_likelihoods", "TestCase", "default_engine", "validate_batch"]
 
 
 def _ptr(a: np.ndarray, typ):
@@ -47,6 +47,17 @@ class _CBatchHolder:
             _ptr(b.base_quals, _lib._u8p), _ptr(b.ins_quals, _lib._u8p),
             _ptr(b.del_quals, _lib._u8p), _ptr(b.gcp_quals, _lib._u8p),
             _ptr(b.read_offsets, _lib._u64p), _ptr(b.read_lengths, _lib._u32p))
+
+
+def validate_batch(b: Batch) -> None:
+    """Checks a batch on the host (no device needed) by the rules the compute
+    calls apply (rodv_batch_validate); raises RodvError with the status a
+    compute call would return and its description."""
+    holder = _CBatchHolder(b)
+    msg = ctypes.create_string_buffer(256)
+    st = _lib.load().rodv_batch_validate(ctypes.byref(holder.c), msg, len(msg))
+    if st != _lib.RODV_OK:
+        raise RodvError(st, msg.value.decode(errors="replace"))
 
 
 class DeviceBatch:

@@ -103,6 +103,8 @@ SIGNATURES = [
     ("rodv_pairhmm_batch", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(CBatch),
                                             ctypes.c_int32, _f64p, ctypes.POINTER(Stats)]),
     ("rodv_batch_num_pairs", ctypes.c_uint64, [ctypes.POINTER(CBatch)]),
+    ("rodv_batch_validate", ctypes.c_int32, [ctypes.POINTER(CBatch), ctypes.c_char_p,
+                                             ctypes.c_size_t]),
     ("rodv_pairhmm_pair", ctypes.c_int32, [ctypes.c_void_p, _u8p, ctypes.c_uint32, _u8p, _u8p,
                                            _u8p, _u8p, _u8p, ctypes.c_uint32, ctypes.c_int32,
                                            _f64p]),

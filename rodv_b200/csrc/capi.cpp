@@ -1,4 +1,5 @@
 // capi.cpp -- extern "C" entry points of include/rodv_pairhmm.h.
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -67,6 +68,18 @@ uint64_t rodv_batch_num_pairs(const rodv_batch* b) {
   for (uint32_t g = 0; g < b->num_regions; ++g)
     n += (uint64_t)b->regions[g].num_haps * b->regions[g].num_reads;
   return n;
+}
+
+rodv_status rodv_batch_validate(const rodv_batch* b, char* msg, size_t msg_len) {
+  if (msg && msg_len) msg[0] = '\0';
+  if (!b) {
+    if (msg && msg_len) snprintf(msg, msg_len, "%s", "null batch");
+    return RODV_ERR_INVALID_ARG;
+  }
+  std::string m;
+  const rodv_status s = rodv::validate_batch(*b, /*check_bases=*/true, nullptr, &m);
+  if (msg && msg_len && s != RODV_OK) snprintf(msg, msg_len, "%s", m.c_str());
+  return s;
 }
 
 rodv_status rodv_pairhmm_batch(rodv_engine* engine, const rodv_batch* batch, int32_t use_double,
