@@ -116,3 +116,61 @@ def test_service_create_without_device_fails_cleanly():
     assert lib.rodv_submit_region(None, None, ctypes.byref(t)) == 1
     assert lib.rodv_poll(None, 1, None, None) == 1
     assert lib.rodv_service_last_error(None) == b""
+
+
+C_CALLER = r"""
+#include <stdio.h>
+#include <string.h>
+#include "rodv_pairhmm.h"
+
+int main(void) {
+  /* one region: two haplotypes x two reads */
+  const char* haps = "ACGTACGTACGTAAAACCCCGGGG";
+  const char* reads = "ACGTAACCCC";
+  const uint64_t hap_off[2] = {0, 12};
+  const uint32_t hap_len[2] = {12, 12};
+  const uint64_t read_off[2] = {0, 5};
+  const uint32_t read_len[2] = {5, 5};
+  uint8_t q[10], gi[10], gc[10];
+  rodv_region reg = {0, 2, 0, 2};
+  rodv_batch b;
+  rodv_options o;
+  rodv_engine* e = NULL;
+  char msg[128];
+  rodv_status s;
+  memset(q, 30, sizeof q); memset(gi, 45, sizeof gi); memset(gc, 10, sizeof gc);
+  b.num_regions = 1; b.regions = &reg;
+  b.num_haps = 2; b.hap_bases = (const uint8_t*)haps; b.hap_offsets = hap_off;
+  b.hap_lengths = hap_len; b.num_reads = 2; b.read_bases = (const uint8_t*)reads;
+  b.base_quals = q; b.ins_quals = gi; b.del_quals = gi; b.gcp_quals = gc;
+  b.read_offsets = read_off; b.read_lengths = read_len;
+  if (rodv_batch_num_pairs(&b) != 4) return 10;
+  if (rodv_batch_validate(&b, msg, sizeof msg) != RODV_OK) return 11;
+  reg.num_reads = 3;                       /* indexes past the read arrays */
+  if (rodv_batch_validate(&b, msg, sizeof msg) != RODV_ERR_INVALID_ARG) return 12;
+  reg.num_reads = 2;
+  rodv_default_options(&o);
+  s = rodv_engine_create(&o, &e);
+  if (s == RODV_OK) rodv_engine_destroy(e);
+  else if (s != RODV_ERR_NO_DEVICE) return 13;
+  printf("%s\n", rodv_status_string(s));
+  return 0;
+}
+"""
+
+
+def test_header_is_c99_and_a_c_caller_links(tmp_path):
+    """A plain C99 caller (gcc -std=c99 -pedantic -Werror) includes the header,
+    builds a batch, validates it and creates an engine (no device here: the
+    clean RODV_ERR_NO_DEVICE status)."""
+    src = tmp_path / "caller.c"
+    src.write_text(C_CALLER)
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-pedantic", "-Wall", "-Wextra", "-Werror",
+                    "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L", libdir, "-l:librodv_pairhmm.so", f"-Wl,-rpath,{libdir}"],
+                   check=True, capture_output=True, text=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert r.stdout.strip() in ("ok", "no usable CUDA device"), r.stdout
