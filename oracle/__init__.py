@@ -39,11 +39,18 @@ _oracle: Optional[ctypes.CDLL] = None
 _ref: Optional[ctypes.CDLL] = None
 
 
+def default_reference_dir() -> str:
+    """The roDV source tree: $RODV_REFERENCE, else a checkout named
+    ``reference`` beside this repository's checkout."""
+    return os.environ.get("RODV_REFERENCE") or os.path.normpath(
+        os.path.join(HERE, "..", "..", "reference"))
+
+
 def build(ref_dir: Optional[str] = None, quiet: bool = True) -> None:
     """Compiles liboracle.so, and the reference library when its tree exists."""
     out = subprocess.DEVNULL if quiet else None
     subprocess.run(["make", "-C", HERE, "oracle"], check=True, stdout=out)
-    ref_dir = ref_dir or "/root/reference"
+    ref_dir = ref_dir or default_reference_dir()
     if os.path.isdir(os.path.join(ref_dir, "src", "core")):
         subprocess.run(["make", "-C", HERE, "ref", f"REF={ref_dir}", "-j8"], check=True,
                        stdout=out)

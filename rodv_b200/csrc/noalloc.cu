@@ -58,8 +58,15 @@ constexpr uint32_t kNaMaxPairs = RODV_NOALLOC_MAX_PAIRS;
 constexpr uint32_t kNaMaxHapLen = RODV_NOALLOC_MAX_HAP_LEN;
 constexpr uint64_t kNaMaxHapBases = RODV_NOALLOC_MAX_HAP_BASES;
 constexpr uint64_t kNaMaxReadBases = RODV_NOALLOC_MAX_READ_BASES;
+// The two forward kernels of this call: the multi-pass FP32 kernel with
+// per-row gap priors and its FP64 rescue.
+using NaF32 = Forward<F32x2, kMaxRowsPerLane, false, true, false, 1>;
+using NaF64 = Forward<F64, kMaxRowsPerLane, false, true, false, 1>;
 constexpr int kNaBlocks = 32;                    // forward kernels' fixed grid
-constexpr int kNaWarps = kNaBlocks * 4;          // resident warps owning boundary rows
+// resident warps owning boundary rows
+constexpr int kNaWarps = kNaBlocks * (NaF32::kWarpsPerBlock > NaF64::kWarpsPerBlock
+                                          ? NaF32::kWarpsPerBlock
+                                          : NaF64::kWarpsPerBlock);
 constexpr uint32_t kNaCols = kNaMaxHapLen + 40;  // boundary columns per warp
 
 constexpr size_t al(size_t v) { return (v + 255) / 256 * 256; }
@@ -88,9 +95,9 @@ constexpr size_t kScratchBytes = al(kOffBoundary + (size_t)kNaWarps * kNaCols * 
 // counter words
 enum : int { kCItems = 0, kCCtr32 = 1, kCCtr64 = 2, kCRescue = 3, kCErr = 4, kCPairs = 5,
              kCHapBytes = 6 };
-// device-side validation bits (bits 0-1 are the forward kernels' ErrorFlag)
+// device-side validation bits (bits 0-3 are the forward kernels' ErrorFlag)
 enum : uint32_t {
-  kNaErrTooMany = 1u << 4,   // pairs / bases above the limits
+  kNaErrTooMany = 1u << 4,   // pairs / bases / one read's length above the limits
   kNaErrHapLen = 1u << 5,    // a haplotype above RODV_NOALLOC_MAX_HAP_LEN
   kNaErrEmpty = 1u << 6,     // a region without haplotypes or reads
   kNaErrIndex = 1u << 7,     // a region indexes outside the batch
@@ -195,7 +202,10 @@ __global__ void __launch_bounds__(1024) na_prefix_kernel(NaArgs a) {
     if (r < b.num_reads) {
       const uint32_t len = b.read_lengths[r];
       if (len == 0) err |= kNaErrZeroLen;
-      v = (len + 3u) & ~3u;
+      // a read above the engine's read limit is refused before its padded
+      // length is formed (64-bit, so no length wraps to a small value)
+      if (len > RODV_MAX_READ_LEN) err |= kNaErrTooMany;
+      v = ((unsigned long long)len + 3ull) & ~3ull;
     }
     unsigned long long ex, agg;
     Scan(tmp).ExclusiveSum(v, ex, agg);
@@ -253,8 +263,8 @@ __global__ void na_pack_kernel(NaArgs a) {
     const uint64_t off = rd[r].row_off;
     const uint32_t len = rd[r].len;
     const uint64_t src = b.read_offsets[r];
-    const uint32_t padded = (len + 3u) & ~3u;
-    for (uint32_t k = lane; k < padded; k += 32) {
+    const uint64_t padded = ((uint64_t)len + 3u) & ~3ull;
+    for (uint64_t k = lane; k < padded; k += 32) {
       uint32_t w = 0;
       if (k < len)
         w = row_word(code_of(b.read_bases[src + k], &err), b.base_quals[src + k],
@@ -307,25 +317,26 @@ __global__ void na_pairs_kernel(NaArgs a) {
 }
 
 // Dynamic shared memory per block of the two kernels.
-constexpr int kSmemF32 = Forward<F32x2, kMaxRowsPerLane, false, true, false, 1>::kWarpsPerBlock *
-                         Forward<F32x2, kMaxRowsPerLane, false, true, false, 1>::kSmemPerWarp;
-constexpr int kSmemF64 = Forward<F64, kMaxRowsPerLane, false, true, false, 1>::kWarpsPerBlock *
-                         Forward<F64, kMaxRowsPerLane, false, true, false, 1>::kSmemPerWarp;
+constexpr int kSmemF32 = NaF32::kWarpsPerBlock * NaF32::kSmemPerWarp;
+constexpr int kSmemF64 = NaF64::kWarpsPerBlock * NaF64::kSmemPerWarp;
 static_assert(kSmemF32 <= 227 * 1024 && kSmemF64 <= 227 * 1024, "tables too large");
 
 // Per-device set-up: the scratch array's device address, tables copied in,
-// the kernels' shared-memory limit raised.
+// the kernels' shared-memory limit raised.  Only a successful set-up is kept:
+// a failed one (say, a call made before the device could be used) is tried
+// again by the next call.
 struct DeviceSlot {
-  std::once_flag once;
   unsigned char* ptr = nullptr;
-  cudaError_t err = cudaSuccess;
 };
 constexpr int kMaxDevices = 64;
 DeviceSlot g_slots[kMaxDevices];
+std::mutex g_setup_mu;
 
 cudaError_t setup_device(int dev, unsigned char** out) {
+  std::lock_guard<std::mutex> lock(g_setup_mu);
   DeviceSlot& slot = g_slots[dev];
-  std::call_once(slot.once, [&] {
+  cudaError_t e = cudaSuccess;
+  if (!slot.ptr) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e == cudaSuccess) {
@@ -347,11 +358,21 @@ cudaError_t setup_device(int dev, unsigned char** out) {
         e = cudaFuncSetAttribute(&forward_kernel<F64, kMaxRowsPerLane, false, true, false, 1>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemF64);
     }
-    slot.err = e;
-    slot.ptr = (e == cudaSuccess) ? static_cast<unsigned char*>(p) : nullptr;
-  });
+    if (e == cudaSuccess) slot.ptr = static_cast<unsigned char*>(p);
+  }
   *out = slot.ptr;
-  return slot.err;
+  return e;
+}
+
+// True when p is memory of the current device (device or managed).
+bool on_device(const void* p, int dev) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();  // an unregistered host pointer; clear the error it left
+    return false;
+  }
+  return (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) &&
+         at.device == dev;
 }
 
 rodv_status status_of_flags(uint32_t f) {
@@ -385,6 +406,17 @@ extern "C" rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return RODV_ERR_NO_DEVICE;
   if (major != 10 || minor != 0) return RODV_ERR_NO_DEVICE;
+  // An error left pending by earlier work on this thread is not this call's
+  // to clear or report as its own: refuse to launch on top of it.
+  if (cudaPeekAtLastError() != cudaSuccess) return RODV_ERR_CUDA;
+  // Every array must be memory of this device: a host pointer read by a
+  // kernel is an illegal access that ends the caller's context.
+  const void* arrays[] = {batch->regions,    batch->hap_bases,  batch->hap_offsets,
+                          batch->hap_lengths, batch->read_bases, batch->base_quals,
+                          batch->ins_quals,  batch->del_quals,  batch->gcp_quals,
+                          batch->read_offsets, batch->read_lengths, out_log10};
+  for (const void* p : arrays)
+    if (!on_device(p, dev)) return RODV_ERR_INVALID_ARG;
   unsigned char* s = nullptr;
   if (setup_device(dev, &s) != cudaSuccess || !s) return RODV_ERR_CUDA;
 
@@ -409,8 +441,8 @@ extern "C" rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32
   v.tab.mm_d = reinterpret_cast<const double*>(s + kOffMmD);
   uint32_t* cnt = reinterpret_cast<uint32_t*>(s + kOffCounters);
 
-  using F32 = Forward<F32x2, kMaxRowsPerLane, false, true, false, 1>;
-  using D64 = Forward<F64, kMaxRowsPerLane, false, true, false, 1>;
+  using F32 = NaF32;
+  using D64 = NaF64;
   ClassLaunch c32{};
   c32.work = s + kOffItems;
   c32.work_count = cnt + kCItems;
@@ -434,6 +466,7 @@ extern "C" rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32
       <<<kNaBlocks, D64::kWarpsPerBlock * kWarp,
          D64::kWarpsPerBlock * D64::kSmemPerWarp, st>>>(
           v, c64);
+  // nothing was pending on entry, so a launch error now is this call's own
   if (cudaGetLastError() != cudaSuccess) return RODV_ERR_CUDA;
 
   uint32_t flags = 0;

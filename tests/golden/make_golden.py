@@ -3,7 +3,7 @@
 Run in a container where the reference tree exists and oracle/_ref is built
 (``make -C oracle REF=<roDV>``):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref PATH_TO_ROOT_OF_roDV]
 
 Fixtures written (all small, all derived from the reference):
 
@@ -147,8 +147,10 @@ def synthetic() -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None,
+                    help="roDV source tree (default: oracle.default_reference_dir())")
     a = ap.parse_args()
+    a.ref = a.ref or oracle.default_reference_dir()
     if not oracle.ref_available():
         oracle.build(a.ref)
     gkl(a.ref)

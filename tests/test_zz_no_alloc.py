@@ -92,3 +92,76 @@ def test_noalloc_fp64_and_limits(engine):
     cb.num_reads = 16385   # above RODV_NOALLOC_MAX_READS: rejected before any launch
     assert lib.rodv_pairhmm_batch_noalloc(ctypes.byref(cb), 0, out.data_ptr(), None) == 7
     del keep
+
+
+def _one_region(L=120, H=300, seed=9):
+    rng = np.random.default_rng(seed)
+    hap = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, H)]
+    read = hap[10:10 + L].copy()
+    q = [rng.integers(10, 41, L).astype(np.uint8), np.full(L, 45, np.uint8),
+         np.full(L, 45, np.uint8), np.full(L, 10, np.uint8)]
+    return Batch.from_regions([([hap, hap[::-1].copy()], [read, read[::-1].copy()], *[[x, x]
+                                                                                    for x in q])])
+
+
+def _faulty(kind):
+    """A small batch with one fault the device-side checks must catch (every
+    array stays in bounds: the checks refuse the batch before any kernel
+    reads past what the caller passed)."""
+    b = _one_region()
+    if kind == "base":          # a base outside A, C, G, T, N
+        b.read_bases[3] = ord("X")
+    elif kind == "empty":       # a region without reads
+        b.regions[0]["num_reads"] = 0
+    elif kind == "index":       # a region indexing past the haplotype array
+        b.regions[0]["num_haps"] = 3
+    elif kind == "zero":        # an empty read
+        b.read_lengths[1] = 0
+    elif kind == "hap_len":     # a haplotype above RODV_NOALLOC_MAX_HAP_LEN
+        rng = np.random.default_rng(3)
+        long_hap = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, 2100)]
+        b = Batch.from_regions([([long_hap], [long_hap[:100].copy()], [np.full(100, 30, np.uint8)],
+                                 [np.full(100, 45, np.uint8)], [np.full(100, 45, np.uint8)],
+                                 [np.full(100, 10, np.uint8)])])
+    elif kind == "read_len":    # one read above RODV_MAX_READ_LEN (65,536 bases)
+        rng = np.random.default_rng(4)
+        L = 70000
+        hap = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, 400)]
+        read = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, L)]
+        b = Batch.from_regions([([hap], [read], [np.full(L, 30, np.uint8)],
+                                 [np.full(L, 45, np.uint8)], [np.full(L, 45, np.uint8)],
+                                 [np.full(L, 10, np.uint8)])])
+    return b
+
+
+# status codes of include/rodv_pairhmm.h
+_EXPECTED = {"base": 3, "empty": 2, "index": 1, "zero": 1, "hap_len": 7, "read_len": 7}
+
+
+def test_noalloc_device_checks_then_valid_call(engine):
+    """Each device-side check maps its fault to the documented status; a host
+    array is refused before any launch; a valid call afterwards still matches
+    rodv_pairhmm_batch."""
+    torch = pytest.importorskip("torch")
+    lib = _lib.load()
+    for kind, status in _EXPECTED.items():
+        b = _faulty(kind)
+        cb, keep = _device_struct(b, torch)
+        n = max(1, int(np.sum(b.regions["num_haps"].astype(np.int64) *
+                              b.regions["num_reads"].astype(np.int64))))
+        out = torch.empty((n,), dtype=torch.float64, device="cuda")
+        st = lib.rodv_pairhmm_batch_noalloc(ctypes.byref(cb), 0, out.data_ptr(), None)
+        assert st == status, (kind, _lib.STATUS_NAMES.get(st, st))
+        del keep
+    # host arrays (what the other entry points take) are refused, nothing launched
+    from rodv_b200 import _CBatchHolder
+    good = _one_region()
+    holder = _CBatchHolder(good)
+    out = torch.empty((good.num_pairs,), dtype=torch.float64, device="cuda")
+    assert lib.rodv_pairhmm_batch_noalloc(ctypes.byref(holder.c), 0, out.data_ptr(), None) == 1
+    # and a valid call still gives the allocating call's results
+    expected = engine.batch(good)
+    cb, keep = _device_struct(good, torch)
+    assert lib.rodv_pairhmm_batch_noalloc(ctypes.byref(cb), 0, out.data_ptr(), None) == 0
+    assert np.abs(out.cpu().numpy() - expected).max() < TOL
+    del keep
