@@ -177,6 +177,41 @@ rodv_status rodv_pairhmm_plain(rodv_engine* engine, rodv_device_batch* dbatch,
 rodv_status rodv_measure_peaks(rodv_engine* engine, double* fp32_gflops, double* fp32x2_gflops,
                                double* fp64_gflops, double* sm_mhz);
 
+/* ---- One batch over several GPUs -------------------------------------------
+ * roDV runs schedule_pairhmm (pairhmm_schedule.cpp:116-340) once per region on
+ * one thread; regions are independent, so a batch splits over GPUs by region
+ * with no exchange between them.  rodv_shard_plan assigns every region to one
+ * of num_shards shards, longest processing time first by cells (sum of
+ * haplotype lengths x sum of read lengths): regions in decreasing cell count,
+ * each to the shard with the fewest cells so far, lowest index on a tie.  The
+ * plan depends only on the batch and num_shards, so every process of a
+ * multi-process job computes the same plan.  Host only: no device is needed.
+ * region_shard receives num_regions shard indices; shard_cells (may be NULL)
+ * num_shards cell counts.
+ * rodv_shard_merge is the inverse step: shard_results[k] holds the results of
+ * shard k's regions, in batch order, as rodv_pairhmm_batch returns them for a
+ * batch of just those regions; they are copied into out_log10 in the batch's
+ * result order.  Host only.
+ * rodv_multi_create makes one engine per listed device (a device may be
+ * listed twice: two engines share it); rodv_multi_batch plans the shards,
+ * runs each device's shard through its engine on its own host thread (host
+ * buffers in and out, as rodv_pairhmm_batch) and merges the results.  Results
+ * are bitwise those of rodv_pairhmm_batch on one device.  stats: pairs,
+ * cells and bytes summed over devices, device times the maximum. */
+rodv_status rodv_shard_plan(const rodv_batch* batch, uint32_t num_shards, uint32_t* region_shard,
+                            uint64_t* shard_cells);
+rodv_status rodv_shard_merge(const rodv_batch* batch, uint32_t num_shards,
+                             const uint32_t* region_shard, const double* const* shard_results,
+                             double* out_log10);
+typedef struct rodv_multi rodv_multi;
+rodv_status rodv_multi_create(const rodv_options* opts, const int32_t* devices,
+                              uint32_t num_devices, rodv_multi** out);
+void rodv_multi_destroy(rodv_multi* multi);
+rodv_status rodv_multi_batch(rodv_multi* multi, const rodv_batch* batch, int32_t use_double,
+                             double* out_log10, rodv_stats* stats);
+/* Details of the last failure of rodv_multi_batch (valid until the next call). */
+const char* rodv_multi_last_error(rodv_multi* multi);
+
 /* ---- Allocation-free batch call ------------------------------------------
  * No counterpart in the reference (roDV computes on the CPU and allocates per
  * call).  For callers that cannot call cudaMalloc: code that owns all device
@@ -188,10 +223,15 @@ rodv_status rodv_measure_peaks(rodv_engine* engine, double* fp32_gflops, double*
  * held by every GPU that loads the library until the process exits.
  *
  * batch: a rodv_batch whose array pointers (regions included) are DEVICE
- * memory on the current device; out_log10: device array of
+ * (or managed) memory on the current device, checked before any launch:
+ * anything else returns RODV_ERR_INVALID_ARG; out_log10: device array of
  * rodv_batch_num_pairs() doubles; stream: a cudaStream_t (NULL = default).
- * Same results as rodv_pairhmm_batch (every pair through the per-row-prior
- * multi-pass kernels).  Returns after the work on `stream` has finished.
+ * Results equal rodv_pairhmm_batch's within 1e-5 log10, not bitwise: this
+ * call sends every pair through the per-row-prior multi-pass kernels, the
+ * batched engine through the scaled and chain kernels.  Returns after the
+ * work on `stream` has finished.  A CUDA error already pending on the
+ * calling thread is left in place and the call returns RODV_ERR_CUDA
+ * without launching.
  * The first call on a device sets that device up (obtains the scratch
  * address, copies the prior tables, raises its two kernels' shared-memory
  * limit per block) and synchronises it: make it before any stream capture.  All calls in a process share the scratch array: calls
@@ -204,7 +244,8 @@ rodv_status rodv_measure_peaks(rodv_engine* engine, double* fp32_gflops, double*
 #define RODV_NOALLOC_MAX_PAIRS 16384u
 #define RODV_NOALLOC_MAX_HAP_LEN 2048u      /* bases per haplotype */
 #define RODV_NOALLOC_MAX_HAP_BASES 1048576u /* bases over all haplotypes */
-#define RODV_NOALLOC_MAX_READ_BASES 1048576u /* bases over all reads */
+#define RODV_NOALLOC_MAX_READ_BASES 1048576u /* bases over all reads; one read at most
+                                                RODV_MAX_READ_LEN bases */
 rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32_t use_double,
                                        double* out_log10, void* stream);
 
@@ -283,6 +324,19 @@ rodv_status rodv_service_get_stats(rodv_service* service, rodv_service_stats* ou
 void rodv_service_reset_stats(rodv_service* service);
 /* Details of the service's last failure (valid until this thread's next call). */
 const char* rodv_service_last_error(rodv_service* service);
+
+/* ---- Testing hooks -----------------------------------------------------------
+ * No counterpart in the reference (whose only failure report is the bool of
+ * schedule_pairhmm, pairhmm_schedule.cpp:130-132).  For tests of the engine's
+ * failure paths without a real out-of-memory condition.
+ * rodv_fault_inject_alloc makes the nth next allocation of one kind fail on
+ * the host exactly as an exhausted cudaMalloc / cudaMallocHost would (kind 0:
+ * device memory, 1: pinned host memory; nth = 0 disarms it).  Process-wide;
+ * affects every engine and service.  rodv_debug_live_allocations reports how
+ * many device and pinned-host allocations of the library are live, so a test
+ * can check that a failed call released what it had allocated. */
+rodv_status rodv_fault_inject_alloc(int32_t kind, int64_t nth);
+void rodv_debug_live_allocations(uint64_t* device, uint64_t* pinned_host);
 
 /* Human-readable name of a status code (static storage). */
 const char* rodv_status_string(rodv_status status);

@@ -26,7 +26,7 @@ from . import _lib
 from ._lib import RodvError
 from .batch import Batch
 
-__all__ = ["Engine", "DeviceBatch", "Service", "Batch", "RodvError", "schedule_pairhmm",
+__all__ = ["Engine", "DeviceBatch", "MultiEngine", "Service", "Batch", "RodvError", "schedule_pairhmm",
            "compute_likelihoods", "TestCase", "default_engine", "validate_batch"]
 
 
@@ -190,6 +190,50 @@ class Engine:
         self._check(self.lib.rodv_measure_peaks(self.h, *[ctypes.byref(x) for x in v]))
         return {"fp32_gflops": v[0].value, "fp32x2_gflops": v[1].value,
                 "fp64_gflops": v[2].value, "sm_mhz": v[3].value}
+
+
+class MultiEngine:
+    """One batch over several devices (rodv_multi): regions sharded by cells,
+    one engine and host thread per device, results merged in batch order;
+    bitwise the results of :meth:`Engine.batch` on one device."""
+
+    def __init__(self, devices: Sequence[int], force_fp64: bool = False, verbose: bool = False):
+        self.lib = _lib.load()
+        opts = _lib.Options()
+        self.lib.rodv_default_options(ctypes.byref(opts))
+        opts.force_fp64 = int(force_fp64)
+        opts.verbose = int(verbose)
+        devs = (ctypes.c_int32 * len(devices))(*devices)
+        h = ctypes.c_void_p()
+        st = self.lib.rodv_multi_create(ctypes.byref(opts), devs, len(devices), ctypes.byref(h))
+        if st != _lib.RODV_OK:
+            detail = self.lib.rodv_last_error(None) or b""
+            raise RodvError(st, "multi-device engine creation failed: " +
+                            detail.decode(errors="replace"))
+        self.h = h
+        self.devices = list(devices)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.rodv_multi_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def batch(self, b: Batch, use_double: bool = False, stats: bool = False):
+        holder = _CBatchHolder(b)
+        out = np.empty(b.num_pairs, dtype=np.float64)
+        st = _lib.Stats()
+        rc = self.lib.rodv_multi_batch(self.h, ctypes.byref(holder.c), int(use_double),
+                                       _ptr(out, _lib._f64p), ctypes.byref(st))
+        if rc != _lib.RODV_OK:
+            raise RodvError(rc, (self.lib.rodv_multi_last_error(self.h) or b"").decode(
+                errors="replace"))
+        return (out, st.as_dict()) if stats else out
 
 
 class Service:

@@ -119,6 +119,17 @@ SIGNATURES = [
     ("rodv_measure_peaks", ctypes.c_int32, [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p]),
     ("rodv_pairhmm_batch_noalloc", ctypes.c_int32, [ctypes.POINTER(CBatch), ctypes.c_int32,
                                                     ctypes.c_void_p, ctypes.c_void_p]),
+    ("rodv_shard_plan", ctypes.c_int32, [ctypes.POINTER(CBatch), ctypes.c_uint32, _u32p,
+                                         _u64p]),
+    ("rodv_shard_merge", ctypes.c_int32, [ctypes.POINTER(CBatch), ctypes.c_uint32, _u32p,
+                                          ctypes.POINTER(_f64p), _f64p]),
+    ("rodv_multi_create", ctypes.c_int32, [ctypes.POINTER(Options),
+                                           ctypes.POINTER(ctypes.c_int32), ctypes.c_uint32,
+                                           ctypes.POINTER(ctypes.c_void_p)]),
+    ("rodv_multi_destroy", None, [ctypes.c_void_p]),
+    ("rodv_multi_batch", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(CBatch),
+                                          ctypes.c_int32, _f64p, ctypes.POINTER(Stats)]),
+    ("rodv_multi_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
     ("rodv_autotune", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int32,
                                        ctypes.POINTER(ctypes.c_int32)]),
     ("rodv_service_create", ctypes.c_int32, [ctypes.POINTER(Options),
@@ -133,6 +144,8 @@ SIGNATURES = [
                                                 ctypes.POINTER(ServiceStats)]),
     ("rodv_service_reset_stats", None, [ctypes.c_void_p]),
     ("rodv_service_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
+    ("rodv_fault_inject_alloc", ctypes.c_int32, [ctypes.c_int32, ctypes.c_int64]),
+    ("rodv_debug_live_allocations", None, [_u64p, _u64p]),
     ("rodv_status_string", ctypes.c_char_p, [ctypes.c_int32]),
     ("rodv_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
 ]

@@ -31,6 +31,17 @@ void rodv_default_options(rodv_options* opts) {
 static std::mutex g_create_mu;
 static std::string g_create_error;
 
+}  // extern "C"
+
+namespace rodv {
+void set_create_error(const std::string& msg) {
+  std::lock_guard<std::mutex> lk(g_create_mu);
+  g_create_error = msg;
+}
+}  // namespace rodv
+
+extern "C" {
+
 rodv_status rodv_engine_create(const rodv_options* opts, rodv_engine** out) {
   if (!out) return RODV_ERR_INVALID_ARG;
   *out = nullptr;
@@ -190,6 +201,16 @@ const char* rodv_status_string(rodv_status s) {
     case RODV_ERR_INTERNAL: return "internal consistency check failed";
     default: return "unknown status";
   }
+}
+
+rodv_status rodv_fault_inject_alloc(int32_t kind, int64_t nth) {
+  if (kind != 0 && kind != 1) return RODV_ERR_INVALID_ARG;
+  rodv::set_alloc_fault(kind, nth);
+  return RODV_OK;
+}
+
+void rodv_debug_live_allocations(uint64_t* device, uint64_t* pinned_host) {
+  rodv::live_allocations(device, pinned_host);
 }
 
 const char* rodv_last_error(rodv_engine* engine) {

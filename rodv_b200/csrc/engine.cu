@@ -36,6 +36,7 @@
 #include <thread>
 
 #include "engine.h"
+#include "trace.h"
 #include "tables.h"
 
 namespace rodv {
@@ -198,28 +199,76 @@ int default_variant(int cls) {
 
 }  // namespace
 
+// Every device and pinned-host allocation of the engine and the service goes
+// through DeviceMem / PinnedMem.  Testing hooks (rodv_fault_inject_alloc,
+// rodv_debug_live_allocations): a countdown per kind makes the n-th next
+// allocation fail on the host, as cudaMalloc / cudaMallocHost fail when memory
+// is exhausted, and live counters show that a failed call released what it
+// had allocated.
+namespace {
+std::atomic<int64_t> g_fail_countdown[2];  // 0: device, 1: pinned host
+std::atomic<int64_t> g_live[2];
+
+bool injected_failure(int kind) {
+  int64_t v = g_fail_countdown[kind].load();
+  while (v > 0)
+    if (g_fail_countdown[kind].compare_exchange_weak(v, v - 1)) return v == 1;
+  return false;
+}
+}  // namespace
+
+void set_alloc_fault(int kind, int64_t nth) { g_fail_countdown[kind].store(nth > 0 ? nth : 0); }
+void live_allocations(uint64_t* device, uint64_t* pinned) {
+  if (device) *device = (uint64_t)g_live[0].load();
+  if (pinned) *pinned = (uint64_t)g_live[1].load();
+}
+
 DeviceMem::~DeviceMem() {
-  if (ptr) cudaFree(ptr);
+  if (ptr) {
+    cudaFree(ptr);
+    --g_live[0];
+  }
 }
 cudaError_t DeviceMem::ensure(size_t n) {
   if (n <= bytes && ptr) return cudaSuccess;
-  if (ptr) cudaFree(ptr);
+  if (ptr) {
+    cudaFree(ptr);
+    --g_live[0];
+  }
   ptr = nullptr;
   bytes = 0;
+  if (injected_failure(0)) return cudaErrorMemoryAllocation;
   cudaError_t e = cudaMalloc(&ptr, std::max<size_t>(n, 1));
-  if (e == cudaSuccess) bytes = n;
+  if (e == cudaSuccess) {
+    bytes = n;
+    ++g_live[0];
+  } else {
+    ptr = nullptr;
+  }
   return e;
 }
 PinnedMem::~PinnedMem() {
-  if (ptr) cudaFreeHost(ptr);
+  if (ptr) {
+    cudaFreeHost(ptr);
+    --g_live[1];
+  }
 }
 cudaError_t PinnedMem::ensure(size_t n) {
   if (n <= bytes && ptr) return cudaSuccess;
-  if (ptr) cudaFreeHost(ptr);
+  if (ptr) {
+    cudaFreeHost(ptr);
+    --g_live[1];
+  }
   ptr = nullptr;
   bytes = 0;
+  if (injected_failure(1)) return cudaErrorMemoryAllocation;
   cudaError_t e = cudaMallocHost(&ptr, std::max<size_t>(n, 1));
-  if (e == cudaSuccess) bytes = n;
+  if (e == cudaSuccess) {
+    bytes = n;
+    ++g_live[1];
+  } else {
+    ptr = nullptr;
+  }
   return e;
 }
 
@@ -399,6 +448,7 @@ rodv_status validate_batch(const rodv_batch& b, bool check_bases, uint64_t* num_
 }
 
 rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64) {
+  TraceRange trace("rodv: pack");
   PackTimer timer(opt_.verbose >= 2);
   plan = PackedPlan{};
   plan.fp64 = fp64;
@@ -1012,6 +1062,7 @@ rodv_status Engine::run_host(const rodv_batch& b, double* out, rodv_stats* st, b
 }
 
 rodv_status Engine::finish_lane(HostLane& l, double* out, rodv_stats* st) {
+  TraceRange trace("rodv: finish range");
   l.busy = false;
   RODV_CUDA(cudaEventSynchronize(l.done));
   if (opt_.verbose >= 2) {

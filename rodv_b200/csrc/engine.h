@@ -43,6 +43,11 @@ enum CounterBlock : int {
   kCountWords = 4 * kNumClasses + 1,
 };
 
+// Testing hooks behind rodv_fault_inject_alloc / rodv_debug_live_allocations:
+// kind 0 = device (cudaMalloc), 1 = pinned host (cudaMallocHost).
+void set_alloc_fault(int kind, int64_t nth);
+void live_allocations(uint64_t* device, uint64_t* pinned);
+
 struct DeviceMem {
   void* ptr = nullptr;
   size_t bytes = 0;
@@ -88,6 +93,9 @@ struct PackedPlan {
   std::vector<uint32_t> hap_len;
   std::vector<uint8_t> read_class;
 };
+
+// Records the message rodv_last_error(NULL) returns (a failed engine creation).
+void set_create_error(const std::string& msg);
 
 // Checks a batch's regions, lengths, limits and (check_bases) every base;
 // the status and message the engine would fail the batch with.

@@ -1,6 +1,7 @@
 // service.cpp -- streaming PairHMM service: continuous batching of submitted
-// regions over two device batch slots (see service.h).
+// regions over three device batch slots (see service.h).
 #include "service.h"
+#include "trace.h"
 
 #include <algorithm>
 #include <cmath>
@@ -249,6 +250,7 @@ void Service::worker() {
 }
 
 rodv_status Service::launch(Slot& s) {
+  TraceRange trace("rodv service: form and launch batch");
   const Clock::time_point t0 = Clock::now();
   // the combined batch: requests' regions, haplotypes and reads back to back
   s.regions.clear();
@@ -292,7 +294,11 @@ rodv_status Service::launch(Slot& s) {
     if (e != cudaSuccess) return engine_.cuda_fail(e, "service staging");
   }
   const Clock::time_point t_stage = Clock::now();
-  rodv_status st = engine_.pack(b, s.plan, s.staging, opt_.force_fp64 != 0);
+  rodv_status st;
+  {
+    TraceRange pack("rodv service: pack");
+    st = engine_.pack(b, s.plan, s.staging, opt_.force_fp64 != 0);
+  }
   if (st != RODV_OK) return st;
   const Clock::time_point t_pack = Clock::now();
   const PackedPlan& p = s.plan;
@@ -321,7 +327,12 @@ rodv_status Service::launch(Slot& s) {
 }
 
 void Service::complete(Slot& s) {
-  const cudaError_t e = cudaEventSynchronize(s.done);
+  cudaError_t e;
+  {
+    TraceRange wait("rodv service: wait for batch");
+    e = cudaEventSynchronize(s.done);
+  }
+  TraceRange trace("rodv service: finish batch");
   if (e != cudaSuccess) {
     fail_slot(s, engine_.cuda_fail(e, "service batch"));
     return;

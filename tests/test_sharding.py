@@ -1,9 +1,11 @@
 """Multi-GPU path on CPU: regions sharded over ranks, no collective on the
-data path, results merged back in batch order.  The ranks here are gloo
-processes on 127.0.0.1 and compute their shard with the CPU oracle (standing
-in for the engine, which needs a GPU); the sharding, the per-rank sub-batch,
-the max-over-ranks timing reduction and the merge are the code bench.py and
-a multi-GPU caller use."""
+data path, results merged back in batch order.  The plan and the merge are
+the library's host-only C entry points (rodv_shard_plan, rodv_shard_merge),
+the same code rodv_multi_batch runs.  The ranks here are gloo processes on
+127.0.0.1 and compute their shard with the CPU oracle (standing in for the
+engine, which needs a GPU); the sharding, the per-rank sub-batch, the
+max-over-ranks timing reduction and the merge are the code bench.py and a
+multi-GPU caller use."""
 import multiprocessing as mp
 import os
 import socket
@@ -25,6 +27,31 @@ def test_lpt_shards_cover_every_region_once_and_balance():
         assert flat == list(range(len(b.regions)))
         loads = [int(cells[s].sum()) for s in shards]
         assert max(loads) - min(loads) <= int(cells.max())
+
+
+def _lpt_reference(cells, world):
+    """Longest processing time first, written out plainly: regions by
+    decreasing cells (stable), each to the least-loaded shard (lowest index on
+    a tie)."""
+    load = [0] * world
+    assign = [0] * len(cells)
+    for g in sorted(range(len(cells)), key=lambda g: -int(cells[g])):
+        k = min(range(world), key=lambda k: (load[k], k))
+        assign[g] = k
+        load[k] += int(cells[g])
+    return assign, load
+
+
+def test_c_plan_is_lpt_by_cells():
+    """rodv_shard_plan (C ABI, host only) against a plain restatement of LPT."""
+    from rodv_b200.sharding import shard_plan
+    b = workloads.make_workload("stream", scale=0.05)
+    cells = region_cells(b)
+    for world in (1, 2, 5):
+        assign, shard_cells = shard_plan(b, world)
+        want, load = _lpt_reference(cells, world)
+        assert assign.tolist() == want
+        assert shard_cells.tolist() == load
 
 
 def test_merge_restores_batch_order():
