@@ -250,14 +250,24 @@ rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32_t use_doub
                                        double* out_log10, void* stream);
 
 /* Autotuner: per work class (read-length bucket and gap-prior form), times
- * every occupancy variant (register budget) of the FP32 kernel on a synthetic
- * batch of that class and keeps the fastest.  With cache_path, a cached
- * result for this device is used unless force != 0, and new results are
- * written there.  variants_out (may be NULL) receives RODV_TUNE_CLASSES
- * variant indices. */
+ * every variant of the class's kernels on a synthetic batch of that class
+ * and keeps the fastest.  Single-pass classes: the FP32 kernel's occupancy
+ * target (register budget) and, for reads up to 128 bases, one or two chain
+ * items per warp.  Multi-pass classes (reads over 256 bases): the strip
+ * height (4 or 8 read rows per lane per pass) and the warps that sweep one
+ * item's passes concurrently (2 or 4), for the FP32 and the FP64 kernel.
+ * Results do not depend on the variants.  No counterpart in the reference,
+ * whose only tunables are the grouping idle ratios of schedule_pairhmm
+ * (pairhmm_schedule.h:23-24), accepted and ignored by the engine's shim.
+ * With cache_path, a cached result for this device is used unless force !=
+ * 0, and new results are written there.  variants_out (may be NULL) receives
+ * the RODV_TUNE_CLASSES FP32 variant indices; rodv_tuned_variants reads the
+ * engine's current FP32 and FP64 variants (either pointer may be NULL). */
 #define RODV_TUNE_CLASSES 18
 rodv_status rodv_autotune(rodv_engine* engine, const char* cache_path, int32_t force,
                           int32_t* variants_out);
+rodv_status rodv_tuned_variants(rodv_engine* engine, int32_t* fp32_variants,
+                                int32_t* fp64_variants);
 
 /* ---- Streaming service -----------------------------------------------------
  * No single counterpart in the reference: it stands for a caller that runs

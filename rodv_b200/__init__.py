@@ -185,6 +185,12 @@ class Engine:
                                            int(force), v))
         return list(v)
 
+    def tuned_variants(self) -> dict:
+        """The engine's current kernel variant per work class, FP32 and FP64."""
+        a, b = (ctypes.c_int32 * 18)(), (ctypes.c_int32 * 18)()
+        self._check(self.lib.rodv_tuned_variants(self.h, a, b))
+        return {"fp32": list(a), "fp64": list(b)}
+
     def measure_peaks(self) -> dict:
         v = [ctypes.c_double() for _ in range(4)]
         self._check(self.lib.rodv_measure_peaks(self.h, *[ctypes.byref(x) for x in v]))

@@ -132,6 +132,8 @@ SIGNATURES = [
     ("rodv_multi_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
     ("rodv_autotune", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int32,
                                        ctypes.POINTER(ctypes.c_int32)]),
+    ("rodv_tuned_variants", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32),
+                                             ctypes.POINTER(ctypes.c_int32)]),
     ("rodv_service_create", ctypes.c_int32, [ctypes.POINTER(Options),
                                              ctypes.POINTER(ctypes.c_void_p)]),
     ("rodv_service_destroy", None, [ctypes.c_void_p]),

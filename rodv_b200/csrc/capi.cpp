@@ -183,6 +183,13 @@ rodv_status rodv_autotune(rodv_engine* engine, const char* cache_path, int32_t f
   return engine->impl->autotune(cache_path, force, variants_out);
 }
 
+rodv_status rodv_tuned_variants(rodv_engine* engine, int32_t* fp32, int32_t* fp64) {
+  if (!engine) return RODV_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(engine->impl->mutex());
+  engine->impl->variants(fp32, fp64);
+  return RODV_OK;
+}
+
 const char* rodv_status_string(rodv_status s) {
   switch (s) {
     case RODV_OK: return "ok";

@@ -36,8 +36,9 @@
 #include <thread>
 
 #include "engine.h"
-#include "trace.h"
 #include "tables.h"
+#include "trace.h"
+#include "worker_pool.h"
 
 namespace rodv {
 
@@ -55,94 +56,6 @@ struct CodeTable {
   }
 };
 const CodeTable kCodes;
-
-// A process-wide pool of host worker threads for the packer.  parallel_for
-// splits [0, n) into chunks of `grain`; the calling thread and up to
-// (chunks - 1) pool workers take chunks until none is left.  Threads are
-// created once: spawning them per call cost more than packing a small batch.
-class WorkerPool {
- public:
-  static WorkerPool& get() {
-    static WorkerPool pool;
-    return pool;
-  }
-  unsigned size() const { return (unsigned)threads_.size(); }
-  void submit(std::function<void()> task) {
-    {
-      std::lock_guard<std::mutex> lk(mu_);
-      tasks_.push_back(std::move(task));
-    }
-    cv_.notify_one();
-  }
-
- private:
-  WorkerPool() {
-    const unsigned n = std::max(1u, std::thread::hardware_concurrency()) - 1;
-    for (unsigned i = 0; i < n; ++i)
-      threads_.emplace_back([this] {
-        for (;;) {
-          std::function<void()> task;
-          {
-            std::unique_lock<std::mutex> lk(mu_);
-            cv_.wait(lk, [&] { return stop_ || !tasks_.empty(); });
-            if (stop_ && tasks_.empty()) return;
-            task = std::move(tasks_.front());
-            tasks_.pop_front();
-          }
-          task();
-        }
-      });
-  }
-  ~WorkerPool() {
-    {
-      std::lock_guard<std::mutex> lk(mu_);
-      stop_ = true;
-    }
-    cv_.notify_all();
-    for (auto& t : threads_) t.join();
-  }
-  std::mutex mu_;
-  std::condition_variable cv_;
-  std::deque<std::function<void()>> tasks_;
-  std::vector<std::thread> threads_;
-  bool stop_ = false;
-};
-
-template <class F>
-void parallel_for(size_t n, size_t grain, F&& f) {
-  const size_t chunks = (n + grain - 1) / grain;
-  const unsigned helpers = (unsigned)std::min<size_t>(WorkerPool::get().size(), chunks ? chunks - 1 : 0);
-  if (helpers == 0) {
-    if (n) f(0, n);
-    return;
-  }
-  struct Job {
-    std::atomic<size_t> next{0};
-    std::atomic<unsigned> running{0};
-    std::mutex mu;
-    std::condition_variable cv;
-  };
-  auto job = std::make_shared<Job>();
-  auto work = [job, chunks, grain, n, &f] {
-    for (;;) {
-      const size_t c = job->next.fetch_add(1);
-      if (c >= chunks) break;
-      f(c * grain, std::min(n, (c + 1) * grain));
-    }
-  };
-  job->running = helpers;
-  for (unsigned t = 0; t < helpers; ++t)
-    WorkerPool::get().submit([job, work] {
-      work();
-      if (job->running.fetch_sub(1) == 1) {
-        std::lock_guard<std::mutex> lk(job->mu);
-        job->cv.notify_all();
-      }
-    });
-  work();
-  std::unique_lock<std::mutex> lk(job->mu);
-  job->cv.wait(lk, [&] { return job->running.load() == 0; });
-}
 
 // Section timer of the packer, printed at verbose level 2.
 struct PackTimer {
@@ -188,14 +101,25 @@ ArenaView arena_view(const PackedPlan& p, uint8_t* base, const PriorTables& tab)
   return a;
 }
 
+// Boundary rows of multi-pass class c (each multi-pass class has its own
+// region: the two classes' kernels run as parallel graph branches).
+float* class_scratch(const PackedPlan& p, const ArenaView& a, int c) {
+  if (!a.scratch || !class_multi(c)) return a.scratch;
+  return reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(a.scratch) +
+                                  (size_t)(c - kSinglePassClasses) * p.scratch_bytes);
+}
+
 // Occupancy variant used before (or without) tuning: the register budget
 // measured best for each rows-per-lane value on B200.
 int default_variant(int cls) {
   const int R = class_rows(cls);
-  if (class_multi(cls) || R >= 3) return 0;  // one chain per warp, 4 blocks/SM (128 registers)
+  if (class_multi(cls)) return 1;            // strip height 8, 4 warps per item
+  if (R >= 3) return 0;                      // one chain per warp, 4 blocks/SM (128 registers)
   if (R == 2) return 4;                      // two 16-lane groups, 4 blocks/SM
   return 6;                                  // two 16-lane groups, 6 blocks/SM (80 registers)
 }
+// FP64 kernels: multi-pass classes have the pipelined variants, the others one.
+int default_variant64(int cls) { return class_multi(cls) ? 1 : 0; }
 
 }  // namespace
 
@@ -273,7 +197,10 @@ cudaError_t PinnedMem::ensure(size_t n) {
 }
 
 Engine::Engine(const rodv_options& opt) : opt_(opt) {
-  for (int c = 0; c < kNumClasses; ++c) variant_[c] = default_variant(c);
+  for (int c = 0; c < kNumClasses; ++c) {
+    variant_[c] = default_variant(c);
+    variant64_[c] = default_variant64(c);
+  }
 }
 
 Engine::~Engine() {
@@ -381,6 +308,21 @@ rodv_status Engine::init() {
     if (s != RODV_OK) return s;
   }
   return RODV_OK;
+}
+
+// Boundary rows a multi-pass class's kernels need: per block of the largest
+// grid any multi-pass kernel variant launches (the autotuner runs every
+// variant on its batches).
+size_t Engine::multi_scratch_rows() const {
+  size_t rows = 0;
+  for (int u = 0; u < 2; ++u)
+    for (int p = 0; p < 3; ++p)
+      for (int v = 0; v < kPipeVariants; ++v) {
+        const Precision pr = p == 2 ? Precision::kF64 : Precision::kF32x2;
+        const KernelInfo k = forward_kernel_info(pr, kMaxRowsPerLane, u != 0, true, p == 0, v);
+        rows = std::max(rows, (size_t)persistent_blocks(k) * k.boundary_rows);
+      }
+  return rows;
 }
 
 // Resident blocks of a kernel on the whole device, queried once per kernel
@@ -595,7 +537,10 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   // kChainHaps) that still leave every resident warp of the class's launch
   // (16 per SM at most) two items; a small batch gets short chains (down to
   // one haplotype).
-  for (int c = 0; c < kNumClasses; ++c) plan.variant[c] = variant_[c];
+  for (int c = 0; c < kNumClasses; ++c) {
+    plan.variant[c] = variant_[c];
+    plan.variant64[c] = variant64_[c];
+  }
   for (int c = 0; c < kSinglePassClasses; ++c) {
     // chain items a warp of this class's kernel sweeps at once
     const int ipw = forward_kernel_info(Precision::kF32x2, class_rows(c), class_uniform(c),
@@ -647,13 +592,17 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       }
     }
   }
-  // Multi-pass leftovers are paired only with leftovers of the same pass
-  // count (a partner with more passes would send this read's last row
-  // through pass-through rows and change its rounding), so a pair's result
-  // does not depend on the rest of the batch.
-  auto passes_of = [&](uint32_t read) { return (b.read_lengths[read] + kPassRows - 1) / kPassRows; };
+  // Multi-pass leftovers are paired with leftovers of the same pass count at
+  // the class's strip height, so neither slot of an item sweeps passes of
+  // pass-through rows only.  (A result does not depend on the partner: the
+  // last pass always ends in pass-through rows, pipe_passes.)
+  auto passes_of = [&](uint32_t read) -> uint32_t {
+    const int c = read_class[read];
+    if (!class_multi(c)) return 1u;  // single-pass leftovers: one group
+    return pipe_passes(b.read_lengths[read], pipe_variant_rows(plan.variant[c]));
+  };
   std::vector<uint64_t> left_by_passes[2];
-  for (int u = 0; u < 2; ++u) left_by_passes[u].assign(RODV_MAX_READ_LEN / kPassRows + 2, 0);
+  for (int u = 0; u < 2; ++u) left_by_passes[u].assign(RODV_MAX_READ_LEN / (kWarp * 4) + 2, 0);
   for (uint32_t g = 0; g < G; ++g)
     for (int u = 0; u < 2; ++u)
       if (left_read[g * 2 + u] != kNoPair)
@@ -709,17 +658,10 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   plan.scratch_cols = plan.multi_max_hap ? plan.multi_max_hap + 40 : 0;
   plan.off_scratch = o;
   if (plan.scratch_cols) {
-    int warps = 0;
-    for (int u = 0; u < 2; ++u)
-      for (int p = 0; p < 3; ++p)
-        for (int v = 0; v < kTuneVariants; ++v) {
-          const Precision pr = p == 2 ? Precision::kF64 : Precision::kF32x2;
-          if (v >= forward_kernel_variants(pr, p == 0, kMaxRowsPerLane, true)) continue;
-          const KernelInfo k = forward_kernel_info(pr, kMaxRowsPerLane, u != 0, true, p == 0, v);
-          warps = std::max(warps, persistent_blocks(k) * k.warps_per_block);
-        }
-    plan.scratch_bytes = (size_t)warps * plan.scratch_cols * 24;
-    o = align_up(o + plan.scratch_bytes);
+    // one region per multi-pass class: the two classes' kernels run as
+    // parallel graph branches and must not share boundary rows
+    plan.scratch_bytes = align_up(multi_scratch_rows() * plan.scratch_cols * 24);
+    o = align_up(o + 2 * plan.scratch_bytes);
   }
   plan.total_bytes = o;
 
@@ -887,8 +829,11 @@ rodv_status Engine::launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, in
   ArenaView a = arena_view(plan, dbase, tab_);
   const uint32_t n = same ? plan.same_items[c] : plan.diff_items[c];
   if (!n) return RODV_OK;
+  // the multi-pass two-haplotype kernel shares the class's variant (strip
+  // height), which the packer paired its items by
   const KernelInfo k = forward_kernel_info(Precision::kF32x2, class_rows(c), class_uniform(c),
-                                           class_multi(c), same, same ? variant : 0);
+                                           class_multi(c), same,
+                                           (same || class_multi(c)) ? variant : 0);
   ClassLaunch cl{};
   cl.work = dbase + (same ? plan.off_same[c] : plan.off_diff[c]);
   cl.work_count = nullptr;
@@ -896,13 +841,35 @@ rodv_status Engine::launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, in
   cl.counter = a.counts + (same ? kCtrSame : kCtrDiff) + c;
   cl.rescue_list = reinterpret_cast<PairRef*>(dbase + plan.off_lists[c]);
   cl.rescue_count = a.counts + kCtrRescue + c;
-  cl.scratch = a.scratch;
+  cl.scratch = class_scratch(plan, a, c);
   cl.scratch_cols = plan.scratch_cols;
   cl.error_flags = a.counts + kCtrError;
-  const int per_block = k.warps_per_block * k.items_per_warp;
+  const int per_block = k.items_per_block;
   const int need = (int)((n + per_block - 1) / per_block);
   int blocks = std::max(1, std::min(persistent_blocks(k), need));
   if (blocks_cap > 0) blocks = std::min(blocks, blocks_cap);
+  void* args[] = {&a.view, &cl};
+  RODV_CUDA(cudaLaunchKernel(k.fn, dim3(blocks), dim3(k.threads), args, k.smem_bytes, stream));
+  return RODV_OK;
+}
+
+// FP64 launch of class c over its list (rescued pairs, or every pair when
+// FP64 is forced); the list's length is read by the kernel.
+rodv_status Engine::launch_fp64_class(const PackedPlan& plan, uint8_t* dbase, int c,
+                                      int variant, cudaStream_t stream) {
+  ArenaView a = arena_view(plan, dbase, tab_);
+  const KernelInfo k = forward_kernel_info(Precision::kF64, class_rows(c), class_uniform(c),
+                                           class_multi(c), false, variant);
+  ClassLaunch cl{};
+  cl.work = dbase + plan.off_lists[c];
+  cl.work_count = a.counts + kCtrRescue + c;
+  cl.static_count = 0;
+  cl.counter = a.counts + kCtrF64 + c;
+  cl.scratch = class_scratch(plan, a, c);
+  cl.scratch_cols = plan.scratch_cols;
+  cl.error_flags = a.counts + kCtrError;
+  const int need = (int)((plan.pairs[c] + k.items_per_block - 1) / k.items_per_block);
+  const int blocks = std::max(1, std::min(persistent_blocks(k), need));
   void* args[] = {&a.view, &cl};
   RODV_CUDA(cudaLaunchKernel(k.fn, dim3(blocks), dim3(k.threads), args, k.smem_bytes, stream));
   return RODV_OK;
@@ -961,22 +928,10 @@ rodv_status Engine::launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stat
   if (parts & 2) RODV_CUDA(fork());
   for (int c = 0; c < kNumClasses && (parts & 2); ++c) {
     if (!plan.pairs[c]) continue;
-    const KernelInfo k =
-        forward_kernel_info(Precision::kF64, class_rows(c), class_uniform(c), class_multi(c));
-    ClassLaunch cl{};
-    cl.work = dbase + plan.off_lists[c];
-    cl.work_count = a.counts + kCtrRescue + c;
-    cl.static_count = 0;
-    cl.counter = a.counts + kCtrF64 + c;
-    cl.scratch = a.scratch;
-    cl.scratch_cols = plan.scratch_cols;
-    cl.error_flags = a.counts + kCtrError;
-    const int need = (int)((plan.pairs[c] + k.warps_per_block - 1) / k.warps_per_block);
-    const int blocks = std::max(1, std::min(persistent_blocks(k), need));
-    void* args[] = {&a.view, &cl};
     const cudaStream_t ls = lane(c);
     if (!ls) return cuda_fail(cudaErrorUnknown, "class stream fork");
-    RODV_CUDA(cudaLaunchKernel(k.fn, dim3(blocks), dim3(k.threads), args, k.smem_bytes, ls));
+    const rodv_status s = launch_fp64_class(plan, dbase, c, plan.variant64[c], ls);
+    if (s != RODV_OK) return s;
     ++launches;
   }
   if (parts & 2) RODV_CUDA(join());
@@ -1377,7 +1332,8 @@ rodv_status Engine::plain(rodv_device_batch* db, double* out, rodv_stats* st) {
           const bool f64 = pass == 1 || plan.fp64;
           const KernelInfo k =
               forward_kernel_info(f64 ? Precision::kF64 : Precision::kF32x2, class_rows(c),
-                                  class_uniform(c), class_multi(c), true, variant_[c]);
+                                  class_uniform(c), class_multi(c), true,
+                                  f64 ? variant64_[c] : variant_[c]);
           ClassLaunch cl{};
           cl.work = f64 ? static_cast<const void*>(w + 32) : static_cast<const void*>(w);
           cl.work_count = nullptr;
@@ -1385,7 +1341,7 @@ rodv_status Engine::plain(rodv_device_batch* db, double* out, rodv_stats* st) {
           cl.counter = f64 ? wc + 1 : wc;
           cl.rescue_list = reinterpret_cast<PairRef*>(w + 32);
           cl.rescue_count = wc + 2;
-          cl.scratch = a.scratch;
+          cl.scratch = class_scratch(plan, a, c);
           cl.scratch_cols = plan.scratch_cols;
           cl.error_flags = wc + 3;
           void* args[] = {&a.view, &cl};
@@ -1419,11 +1375,17 @@ rodv_status Engine::plain(rodv_device_batch* db, double* out, rodv_stats* st) {
 }
 
 // ---------------------------------------------------------------------------
-// Autotuning: per work class, the occupancy variant (register budget) of the
-// same-haplotype FP32 kernel (chain kernel for single-pass classes), chosen by
-// timing every variant on a synthetic batch of that class (reads of 32R-5
-// bases, or 700 for multi-pass, against four 400- or 1,200-base haplotypes
-// per region).  Results are cached per device.
+// Autotuning.  Per work class, every variant of the class's FP32 kernel is
+// timed on a synthetic batch of that class and the fastest kept:
+//   single-pass classes: the occupancy target (blocks per SM, which caps the
+//     registers) and, for reads up to 128 bases, one or two chain items per
+//     warp (16-lane groups with twice the rows per lane);
+//   multi-pass classes: the strip height (4 or 8 rows per lane per pass) and
+//     the warps that sweep one item's passes concurrently (2 or 4), for the
+//     FP32 kernel and, on a batch forced to FP64, for the FP64 kernel.
+// Synthetic batches: reads of 32R-5 bases against four 400-base haplotypes
+// per region (single-pass), or 1,500-base reads against 3,000-base
+// haplotypes (multi-pass).  Results are cached per device.
 // ---------------------------------------------------------------------------
 std::string Engine::device_key() const {
   std::string k = device_name_;
@@ -1440,12 +1402,18 @@ bool Engine::load_tuning(const std::string& path) {
   while (std::getline(in, line)) {
     std::istringstream ss(line);
     std::string k;
-    int c, v;
-    if (!(ss >> k >> c >> v) || k != key) continue;
-    if (c >= 0 && c < kNumClasses && v >= 0 && v < kTuneVariants) {
-      variant_[c] = v;
-      ++found;
-    }
+    int c, v, v64;
+    if (!(ss >> k >> c >> v >> v64) || k != key) continue;
+    if (c < 0 || c >= kNumClasses) continue;
+    if (v < 0 ||
+        v >= forward_kernel_variants(Precision::kF32x2, true, class_rows(c), class_multi(c)))
+      continue;
+    if (v64 < 0 ||
+        v64 >= forward_kernel_variants(Precision::kF64, false, class_rows(c), class_multi(c)))
+      continue;
+    variant_[c] = v;
+    variant64_[c] = v64;
+    ++found;
   }
   tuned_ = found == kNumClasses;
   return tuned_;
@@ -1454,9 +1422,68 @@ bool Engine::load_tuning(const std::string& path) {
 bool Engine::save_tuning(const std::string& path) const {
   std::ofstream out(path, std::ios::trunc);
   if (!out) return false;
-  for (int c = 0; c < kNumClasses; ++c) out << device_key() << ' ' << c << ' ' << variant_[c] << '\n';
+  for (int c = 0; c < kNumClasses; ++c)
+    out << device_key() << ' ' << c << ' ' << variant_[c] << ' ' << variant64_[c] << '\n';
   return (bool)out;
 }
+
+namespace {
+// What a kernel variant is, for the tuner's log.
+std::string variant_name(int cls, int v, bool fp64) {
+  char buf[96];
+  if (class_multi(cls))
+    snprintf(buf, sizeof(buf), "strip height %d, %d warps per item", pipe_variant_rows(v),
+             pipe_variant_warps(v));
+  else if (fp64)
+    snprintf(buf, sizeof(buf), "one variant");
+  else
+    snprintf(buf, sizeof(buf), "%d blocks/SM%s", kVariantMinBlocks[v],
+             v >= kOccupancyTargets ? ", two 16-lane chains per warp" : "");
+  return buf;
+}
+
+// A synthetic batch of one work class (the tuner's input).
+struct TuneBatch {
+  std::vector<uint8_t> hb, rb, q, ins, del, gcp;
+  std::vector<uint64_t> ho, ro;
+  std::vector<uint32_t> hl, rl;
+  std::vector<rodv_region> rg;
+  rodv_batch view() const {
+    return rodv_batch{(uint32_t)rg.size(), rg.data(), (uint32_t)hl.size(), hb.data(),
+                      ho.data(), hl.data(), (uint32_t)rl.size(), rb.data(), q.data(),
+                      ins.data(), del.data(), gcp.data(), ro.data(), rl.data()};
+  }
+};
+
+void make_tune_batch(TuneBatch& tb, std::mt19937& rng, int regions, int haps, int reads,
+                     uint32_t H, uint32_t L, bool uni) {
+  const char* acgt = "ACGT";
+  for (int g = 0; g < regions; ++g) {
+    rodv_region r{(uint32_t)tb.ho.size(), (uint32_t)haps, (uint32_t)tb.ro.size(),
+                  (uint32_t)reads};
+    std::string base;
+    for (uint32_t j = 0; j < H; ++j) base += acgt[rng() % 4];
+    for (int h = 0; h < haps; ++h) {
+      tb.ho.push_back(tb.hb.size());
+      tb.hl.push_back(H);
+      for (uint32_t j = 0; j < H; ++j) tb.hb.push_back(rng() % 100 ? base[j] : acgt[rng() % 4]);
+    }
+    for (int k = 0; k < reads; ++k) {
+      tb.ro.push_back(tb.rb.size());
+      tb.rl.push_back(L);
+      const uint32_t st = rng() % (H - std::min(L, H) + 1);
+      for (uint32_t j = 0; j < L; ++j) {
+        tb.rb.push_back(j + st < H && rng() % 100 ? base[j + st] : acgt[rng() % 4]);
+        tb.q.push_back(10 + rng() % 31);
+        tb.ins.push_back(uni ? 45 : 20 + rng() % 26);
+        tb.del.push_back(uni ? 45 : 20 + rng() % 26);
+        tb.gcp.push_back(uni ? 10 : 5 + rng() % 11);
+      }
+    }
+    tb.rg.push_back(r);
+  }
+}
+}  // namespace
 
 rodv_status Engine::autotune(const char* cache_path, int force, int32_t* variants_out) {
   const std::string path = cache_path ? cache_path : "";
@@ -1467,90 +1494,92 @@ rodv_status Engine::autotune(const char* cache_path, int force, int32_t* variant
   }
   RODV_CUDA(cudaSetDevice(device_));
   std::mt19937 rng(12345);
-  const char* acgt = "ACGT";
+  // Times `launch` (three runs, the first discarded) after a counter reset.
+  auto time_launch = [&](const PackedPlan& plan, uint8_t* d, const auto& launch,
+                         float* best) -> rodv_status {
+    *best = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+      RODV_CUDA(cudaMemsetAsync(d + plan.off_counts, 0, kCountWords * 4, stream_));
+      if (plan.fp64)
+        RODV_CUDA(cudaMemcpyAsync(d + plan.off_counts + kCtrRescue * 4, d + plan.off_preset,
+                                  kNumClasses * 4, cudaMemcpyDeviceToDevice, stream_));
+      RODV_CUDA(cudaEventRecord(ev_[0], stream_));
+      const rodv_status s = launch();
+      if (s != RODV_OK) return s;
+      RODV_CUDA(cudaEventRecord(ev_[1], stream_));
+      RODV_CUDA(cudaEventSynchronize(ev_[1]));
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+      if (rep > 0) *best = std::min(*best, ms);
+    }
+    return check_errors(plan, d);
+  };
   for (int c = 0; c < kNumClasses; ++c) {
     const int R = class_rows(c);
     const bool multi = class_multi(c), uni = class_uniform(c);
-    const uint32_t L = multi ? 700 : (uint32_t)std::max(1, 32 * R - 5);
-    const uint32_t H = multi ? 1200 : 400;
-    // Enough items that every warp of the largest grid takes several (chain
-    // items of 4 haplotypes: ~8; multi-pass same-haplotype items: ~4), so the
-    // timing reflects per-item throughput and not the tail of the work queue.
-    const uint64_t max_warps = (uint64_t)num_sms_ * kVariantMinBlocks[kTuneVariants - 1] * 4;
-    const int regions = 16, haps = 4;
-    const uint64_t items = max_warps * (multi ? 4 : 8);
-    const int reads = (int)std::max<uint64_t>(
-        2, (multi ? 2 * items / (regions * haps) : 2 * items / regions) + 1);
-    std::vector<uint8_t> hb, rb, q, ins, del, gcp;
-    std::vector<uint64_t> ho, ro;
-    std::vector<uint32_t> hl, rl;
-    std::vector<rodv_region> rg;
-    for (int g = 0; g < regions; ++g) {
-      rodv_region r{(uint32_t)ho.size(), (uint32_t)haps, (uint32_t)ro.size(), (uint32_t)reads};
-      std::string base;
-      for (uint32_t j = 0; j < H; ++j) base += acgt[rng() % 4];
-      for (int h = 0; h < haps; ++h) {
-        ho.push_back(hb.size());
-        hl.push_back(H);
-        for (uint32_t j = 0; j < H; ++j) hb.push_back(rng() % 100 ? base[j] : acgt[rng() % 4]);
-      }
-      for (int k = 0; k < reads; ++k) {
-        ro.push_back(rb.size());
-        rl.push_back(L);
-        const uint32_t st = rng() % (H - std::min(L, H) + 1);
-        for (uint32_t j = 0; j < L; ++j) {
-          rb.push_back(j + st < H && rng() % 100 ? base[j + st] : acgt[rng() % 4]);
-          q.push_back(10 + rng() % 31);
-          ins.push_back(uni ? 45 : 20 + rng() % 26);
-          del.push_back(uni ? 45 : 20 + rng() % 26);
-          gcp.push_back(uni ? 10 : 5 + rng() % 11);
-        }
-      }
-      rg.push_back(r);
+    TuneBatch tb;
+    if (multi) {
+      // long pairs: several waves of the largest grid of one item per block
+      make_tune_batch(tb, rng, num_sms_ * 4, 1, 2, 3000, 1500, uni);
+    } else {
+      // Enough items that every warp of the largest grid takes several (chain
+      // items of 4 haplotypes: ~8), so the timing reflects per-item throughput
+      // and not the tail of the work queue.
+      const uint64_t max_warps = (uint64_t)num_sms_ * kVariantMinBlocks[kTuneVariants - 1] * 4;
+      const int regions = 16;
+      const int reads = (int)std::max<uint64_t>(2, 2 * max_warps * 8 / regions + 1);
+      make_tune_batch(tb, rng, regions, 4, reads, 400, (uint32_t)std::max(1, 32 * R - 5), uni);
     }
-    rodv_batch b{(uint32_t)rg.size(), rg.data(), (uint32_t)hl.size(), hb.data(), ho.data(),
-                 hl.data(), (uint32_t)rl.size(), rb.data(), q.data(), ins.data(), del.data(),
-                 gcp.data(), ro.data(), rl.data()};
-    rodv_device_batch* db = nullptr;
-    rodv_status s = upload(b, &db);
-    if (s != RODV_OK) return s;
-    uint8_t* d = static_cast<uint8_t*>(db->arena.ptr);
-    const uint32_t* counts = reinterpret_cast<const uint32_t*>(d + db->plan.off_counts);
-    float best_ms = 1e30f;
-    int best_v = variant_[c];
-    const int nvar = forward_kernel_variants(Precision::kF32x2, true, R, multi);
-    for (int v = 0; v < nvar; ++v) {
-      float vbest = 1e30f;
-      for (int rep = 0; rep < 3; ++rep) {
-        RODV_CUDA(cudaMemsetAsync((void*)counts, 0, kCountWords * 4, stream_));
-        RODV_CUDA(cudaEventRecord(ev_[0], stream_));
-        s = launch_fp32_class(db->plan, d, c, true, v, 0, stream_);
+    const rodv_batch b = tb.view();
+    for (int prec = 0; prec < (multi ? 2 : 1); ++prec) {
+      const bool f64 = prec == 1;
+      auto* db = new rodv_device_batch();
+      PinnedMem staging;
+      rodv_status s = pack(b, db->plan, staging, f64);
+      cudaError_t e = s == RODV_OK ? db->arena.ensure(db->plan.total_bytes) : cudaSuccess;
+      if (s == RODV_OK && e == cudaSuccess)
+        e = cudaMemcpyAsync(db->arena.ptr, staging.ptr, db->plan.upload_bytes,
+                            cudaMemcpyHostToDevice, stream_);
+      if (s != RODV_OK || e != cudaSuccess) {
+        delete db;
+        return s != RODV_OK ? s : cuda_fail(e, "tuning batch upload");
+      }
+      uint8_t* d = static_cast<uint8_t*>(db->arena.ptr);
+      const Precision pr = f64 ? Precision::kF64 : Precision::kF32x2;
+      const int nvar = forward_kernel_variants(pr, !f64, R, multi);
+      int* slot = f64 ? &variant64_[c] : &variant_[c];
+      float best_ms = 1e30f;
+      int best_v = *slot;
+      for (int v = 0; v < nvar; ++v) {
+        float ms = 0.f;
+        s = time_launch(
+            db->plan, d,
+            [&]() {
+              return f64 ? launch_fp64_class(db->plan, d, c, v, stream_)
+                         : launch_fp32_class(db->plan, d, c, true, v, 0, stream_);
+            },
+            &ms);
         if (s != RODV_OK) {
           delete db;
           return s;
         }
-        RODV_CUDA(cudaEventRecord(ev_[1], stream_));
-        RODV_CUDA(cudaEventSynchronize(ev_[1]));
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
-        if (rep > 0) vbest = std::min(vbest, ms);
+        if (opt_.verbose)
+          fprintf(stderr, "rodv: tune %s class %d (R=%d%s%s) variant %d (%s): %.3f ms\n",
+                  f64 ? "FP64" : "FP32", c, R, uni ? ", uniform" : "",
+                  multi ? ", multi-pass" : "", v, variant_name(c, v, f64).c_str(), ms);
+        if (ms < best_ms) {
+          best_ms = ms;
+          best_v = v;
+        }
       }
+      delete db;
+      *slot = best_v;
       if (opt_.verbose)
-        fprintf(stderr, "rodv: tune class %d R=%d%s%s variant %d (%d blocks/SM): %.3f ms\n", c,
-                R, uni ? " uniform" : "", multi ? " multi" : "", v, kVariantMinBlocks[v], vbest);
-      if (vbest < best_ms) {
-        best_ms = vbest;
-        best_v = v;
-      }
+        fprintf(stderr, "rodv: tuned %s class %d (R=%d%s%s): variant %d (%s), %.3f ms\n",
+                f64 ? "FP64" : "FP32", c, R, uni ? ", uniform" : "",
+                multi ? ", multi-pass" : "", best_v, variant_name(c, best_v, f64).c_str(),
+                best_ms);
     }
-    s = check_errors(db->plan, d);
-    delete db;
-    if (s != RODV_OK) return s;
-    variant_[c] = best_v;
-    if (opt_.verbose)
-      fprintf(stderr, "rodv: tuned class %d (R=%d%s%s): %d blocks/SM, %.3f ms\n", c, R,
-              uni ? ", uniform" : "", multi ? ", multi-pass" : "", kVariantMinBlocks[best_v],
-              best_ms);
   }
   tuned_ = true;
   if (!path.empty()) save_tuning(path);

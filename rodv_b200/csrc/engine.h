@@ -77,6 +77,7 @@ struct PackedPlan {
   uint32_t diff_items[kNumClasses] = {};   // FP32 two-haplotype items (multi-pass leftovers)
   uint32_t chain_haps[kNumClasses] = {};   // haplotypes per chain item (single-pass classes)
   int variant[kNumClasses] = {};           // kernel variant per class the items were packed for
+  int variant64[kNumClasses] = {};         // FP64 kernel variant per class
   uint32_t pairs[kNumClasses] = {};        // pairs per class (FP64 list capacity)
   size_t off_hap_codes = 0, off_read_rows = 0, off_haps = 0, off_reads = 0;
   size_t off_same[kNumClasses] = {};
@@ -119,6 +120,13 @@ class Engine {
   rodv_status plain(rodv_device_batch* db, double* out, rodv_stats* st);
   rodv_status measure_peaks(double* f32, double* f32x2, double* f64, double* mhz);
   rodv_status autotune(const char* cache_path, int force, int32_t* variants_out);
+  // The current FP32 and FP64 kernel variant of every class (either may be null).
+  void variants(int32_t* fp32, int32_t* fp64) const {
+    for (int c = 0; c < kNumClasses; ++c) {
+      if (fp32) fp32[c] = variant_[c];
+      if (fp64) fp64[c] = variant64_[c];
+    }
+  }
 
   std::mutex& mutex() { return mu_; }
   // One stage of the chunked host-buffer path: a region range packed,
@@ -152,12 +160,15 @@ class Engine {
                          bool fan_out = false);
   rodv_status launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, int cls, bool same,
                                 int variant, int blocks_cap, cudaStream_t stream);
+  rodv_status launch_fp64_class(const PackedPlan& plan, uint8_t* dbase, int cls, int variant,
+                                cudaStream_t stream);
   rodv_status check_errors(const PackedPlan& plan, uint8_t* dbase);
   rodv_status run_host_single(const rodv_batch& b, double* out, rodv_stats* st, bool fp64);
   rodv_status run_host_chunked(const rodv_batch& b, double* out, rodv_stats* st, bool fp64,
                                const std::vector<uint32_t>& bounds);
   rodv_status finish_lane(HostLane& lane, double* out, rodv_stats* st);
   int persistent_blocks(const KernelInfo& k) const;
+  size_t multi_scratch_rows() const;
   std::string device_key() const;
   bool load_tuning(const std::string& path);
   bool save_tuning(const std::string& path) const;
@@ -174,7 +185,8 @@ class Engine {
   cudaEvent_t fork_ev_ = nullptr, join_ev_[kNumClasses] = {};
   DeviceMem tables_;
   PriorTables tab_{};
-  int variant_[kNumClasses] = {};          // tuned occupancy variant per class
+  int variant_[kNumClasses] = {};          // tuned FP32 kernel variant per class
+  int variant64_[kNumClasses] = {};        // tuned FP64 kernel variant per class
   bool tuned_ = false;
   // buffers of the one-call path (rodv_pairhmm_batch), reused across calls
   PinnedMem staging_;

@@ -1,12 +1,14 @@
 // kernel_table.cuh -- KernelInfo of every forward-kernel instantiation.
 //
 // Each rows-per-lane value R is instantiated in its own translation unit
-// (kernels_r<R>.cu, kernels_multi.cu) so the ~100 kernels compile in parallel.
+// (kernels_r<R>.cu; multi-pass strip heights in kernels_multi_r<R>.cu) so the
+// ~150 kernels compile in parallel.
 #pragma once
 #include <type_traits>
 
 #include "kernels.h"
 #include "pairhmm_fwd.cuh"
+#include "pairhmm_pipe.cuh"
 
 namespace rodv {
 
@@ -23,9 +25,57 @@ KernelInfo make_info(int variant) {
   k.same_hap = SAME || P::kSlots == 1;
   k.chain = F::kChain;
   k.items_per_warp = F::kGroups;
+  k.items_per_block = F::kWarpsPerBlock * F::kGroups;
   k.min_blocks = MINB;
   k.variant = variant;
   return k;
+}
+
+// Multi-pass kernels: the passes of one item on the W warps of a block.
+template <class P, int R, bool U, bool SAME, int W>
+KernelInfo make_pipe_info(int variant) {
+  using F = PipeForward<P, R, U, SAME, 1, W>;
+  KernelInfo k;
+  k.fn = reinterpret_cast<const void*>(&forward_pipe_kernel<P, R, U, SAME, 1, W>);
+  k.threads = W * kWarp;
+  k.warps_per_block = W;
+  k.smem_bytes = W * F::kSmemPerWarp;
+  k.rows_per_lane = R;
+  k.multi = true;
+  k.same_hap = SAME || P::kSlots == 1;
+  k.chain = false;
+  k.items_per_warp = 1;
+  k.items_per_block = 1;
+  k.min_blocks = 1;
+  k.boundary_rows = F::kRows;
+  k.variant = variant;
+  return k;
+}
+
+// The multi-pass variants of strip height R (pipe_variant_rows) for one
+// precision and item kind: W = 2 or 4 warps per item.
+template <int R>
+KernelInfo pipe_info_for(Precision prec, bool uniform, bool same, int variant) {
+  const bool w4 = pipe_variant_warps(variant) == 4;
+  if (prec == Precision::kF64) {
+    if (uniform)
+      return w4 ? make_pipe_info<F64, R, true, false, 4>(variant)
+                : make_pipe_info<F64, R, true, false, 2>(variant);
+    return w4 ? make_pipe_info<F64, R, false, false, 4>(variant)
+              : make_pipe_info<F64, R, false, false, 2>(variant);
+  }
+  if (same) {
+    if (uniform)
+      return w4 ? make_pipe_info<F32x2, R, true, true, 4>(variant)
+                : make_pipe_info<F32x2, R, true, true, 2>(variant);
+    return w4 ? make_pipe_info<F32x2, R, false, true, 4>(variant)
+              : make_pipe_info<F32x2, R, false, true, 2>(variant);
+  }
+  if (uniform)
+    return w4 ? make_pipe_info<F32x2, R, true, false, 4>(variant)
+              : make_pipe_info<F32x2, R, true, false, 2>(variant);
+  return w4 ? make_pipe_info<F32x2, R, false, false, 4>(variant)
+            : make_pipe_info<F32x2, R, false, false, 2>(variant);
 }
 
 // Same-haplotype FP32 kernels come in occupancy targets (kVariantMinBlocks);

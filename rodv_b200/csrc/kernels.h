@@ -16,9 +16,18 @@ struct KernelInfo {
   bool same_hap = false;      // both pairs of an item share the haplotype
   bool chain = false;         // takes ChainItem work (single-pass same-haplotype FP32)
   int items_per_warp = 1;     // chain items a warp sweeps at once (one per lane group)
+  int items_per_block = 1;    // work items a block has in flight
   int min_blocks = 1;         // launch-bounds occupancy target (caps registers)
+  int boundary_rows = 0;      // multi-pass: boundary rows of scratch per block of the grid
   int variant = 0;
 };
+
+// Multi-pass (pipelined) kernels: a variant is a strip height R (rows per
+// lane per pass: 8 or 4) and the warps W of a block that sweep one item's
+// passes concurrently (2 or 4).
+constexpr int kPipeVariants = 4;
+inline int pipe_variant_rows(int variant) { return (variant & 2) ? 4 : 8; }
+inline int pipe_variant_warps(int variant) { return (variant & 1) ? 4 : 2; }
 
 // Variants of the tunable (same-haplotype FP32) kernels: an occupancy target
 // (blocks per SM, which caps registers) and, for the chain kernels of reads
@@ -30,19 +39,23 @@ constexpr int kOccupancyTargets = 4;
 constexpr int kVariantMinBlocks[kTuneVariants] = {4, 5, 6, 8, 4, 5, 6, 8};
 constexpr int kMaxGroupedRows = 4;  // classes with R <= 4 have the grouped variants
 
-// Forward kernel for one work class.  rows_per_lane in 1..8; multi kernels
-// always use 8 rows per lane.  same: FP32 items whose reads share the
-// haplotypes -- ChainItem for single-pass classes, SameItem for multi-pass
-// ones; !same: DiffItem (multi-pass leftovers; in a single-pass class, the
-// pairs of each region's odd read).
-// FP64 kernels take PairRef lists.  variant < forward_kernel_variants(...)
-// selects the variant of same-haplotype FP32 kernels.
+// Forward kernel for one work class.  rows_per_lane in 1..8 for single-pass
+// kernels; multi-pass kernels take their strip height from the variant.
+// same: FP32 items whose reads share the haplotypes -- ChainItem for
+// single-pass classes, SameItem for multi-pass ones; !same: DiffItem
+// (multi-pass leftovers; in a single-pass class, the pairs of each region's
+// odd read).  FP64 kernels take PairRef lists.  variant <
+// forward_kernel_variants(...) selects the variant: of same-haplotype FP32
+// single-pass kernels, and of every multi-pass kernel (FP32 same and
+// two-haplotype items share the class's variant, so they agree on the pass
+// count; FP64 ones have their own).
 KernelInfo forward_kernel_info(Precision prec, int rows_per_lane, bool uniform, bool multi,
                                bool same = true, int variant = 0);
 inline int forward_kernel_variants(Precision prec, bool same, int rows_per_lane = 8,
                                    bool multi = true) {
+  if (multi) return kPipeVariants;
   if (prec != Precision::kF32x2 || !same) return 1;
-  return (!multi && rows_per_lane <= kMaxGroupedRows) ? kTuneVariants : kOccupancyTargets;
+  return rows_per_lane <= kMaxGroupedRows ? kTuneVariants : kOccupancyTargets;
 }
 
 // Peak microbenchmarks: kind 0 = FP32 FFMA, 1 = FP32x2 FFMA2, 2 = FP64 DFMA.

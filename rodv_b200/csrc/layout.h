@@ -105,6 +105,12 @@ struct DiffItem {
   PairRef y;
 };
 
+// Passes of a multi-pass sweep of a read of `len` rows with R rows per lane:
+// floor(len / 32R) + 1, so the last pass always ends in pass-through rows.
+RODV_HD inline uint32_t pipe_passes(uint32_t len, int rows_per_lane) {
+  return len / (uint32_t)(kWarp * rows_per_lane) + 1u;
+}
+
 RODV_HD inline uint32_t row_word(uint32_t code, uint32_t q, uint32_t ins,
                                              uint32_t del, uint32_t gcp) {
   return (code & 7u) | ((q & 127u) << 3) | ((ins & 127u) << 10) | ((del & 127u) << 17) |
@@ -155,6 +161,7 @@ enum ErrorFlag : uint32_t {
   kErrPassLimit = 2u,   // a read longer than the pass limit reached a kernel
   kErrChain = 4u,       // a chain item with no haplotypes
   kErrNonFinite = 8u,   // a likelihood came out NaN or infinite (an arithmetic fault)
+  kErrWaitTimeout = 16u,  // a pipelined sweep waited too long for another warp's progress
 };
 
 }  // namespace rodv

@@ -95,14 +95,14 @@ constexpr size_t kScratchBytes = al(kOffBoundary + (size_t)kNaWarps * kNaCols * 
 // counter words
 enum : int { kCItems = 0, kCCtr32 = 1, kCCtr64 = 2, kCRescue = 3, kCErr = 4, kCPairs = 5,
              kCHapBytes = 6 };
-// device-side validation bits (bits 0-3 are the forward kernels' ErrorFlag)
+// device-side validation bits (the low bits are the forward kernels' ErrorFlag)
 enum : uint32_t {
-  kNaErrTooMany = 1u << 4,   // pairs / bases / one read's length above the limits
-  kNaErrHapLen = 1u << 5,    // a haplotype above RODV_NOALLOC_MAX_HAP_LEN
-  kNaErrEmpty = 1u << 6,     // a region without haplotypes or reads
-  kNaErrIndex = 1u << 7,     // a region indexes outside the batch
-  kNaErrZeroLen = 1u << 8,   // an empty haplotype or read
-  kNaErrBase = 1u << 9,      // a base other than A, C, G, T, N
+  kNaErrTooMany = 1u << 8,   // pairs / bases / one read's length above the limits
+  kNaErrHapLen = 1u << 9,    // a haplotype above RODV_NOALLOC_MAX_HAP_LEN
+  kNaErrEmpty = 1u << 10,    // a region without haplotypes or reads
+  kNaErrIndex = 1u << 11,    // a region indexes outside the batch
+  kNaErrZeroLen = 1u << 12,  // an empty haplotype or read
+  kNaErrBase = 1u << 13,     // a base other than A, C, G, T, N
 };
 
 // The scratch array.  In host code this name is a host-side stand-in, not a

@@ -561,6 +561,22 @@ struct Forward {
                                         const BoundaryCell* buf, const uint32_t (&H)[2],
                                         const uint32_t (&L)[2], uint32_t row, int lane,
                                         uint32_t item) {
+    const bool rejected = row_bound_rejects(b, c, buf, H, L, row, lane, item);
+    if (rejected && lane == 0) {
+      PairRef refs[2];
+      load_refs(c, item, refs);
+      finish(b, c, refs[0], 0.0);
+      if (refs[1].read != kNoPair) finish(b, c, refs[1], 0.0);
+    }
+    return rejected;
+  }
+
+  // The decision of sweep_rejected, taken by the whole warp (the same value
+  // in every lane); nothing is written.
+  __device__ static bool row_bound_rejects(const BatchView& b, const ClassLaunch& c,
+                                           const BoundaryCell* buf, const uint32_t (&H)[2],
+                                           const uint32_t (&L)[2], uint32_t row, int lane,
+                                           uint32_t item) {
     V sm = P::zero(), si = P::zero();
     for (uint32_t col = 1 + (uint32_t)lane; col <= H[0]; col += kWarp) {
       const BoundaryCell cell = buf[col];
@@ -598,10 +614,6 @@ struct Forward {
         bound = sum_m[s] + sum_i[s];
       }
       rejected = rejected && bound >= 0.0 && bound < amin * 1e-6;
-    }
-    if (rejected && lane == 0) {
-      finish(b, c, refs[0], 0.0);
-      if (refs[1].read != kNoPair) finish(b, c, refs[1], 0.0);
     }
     return rejected;
   }

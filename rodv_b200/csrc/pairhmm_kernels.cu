@@ -10,10 +10,16 @@ namespace rodv {
 
 template <int R, bool MU>
 KernelInfo info_for(Precision prec, bool uniform, bool same, int variant);
+template <int R>
+KernelInfo pipe_info_for(Precision prec, bool uniform, bool same, int variant);
 
 KernelInfo forward_kernel_info(Precision prec, int rows_per_lane, bool uniform, bool multi,
                                bool same, int variant) {
-  if (multi) return info_for<kMaxRowsPerLane, true>(prec, uniform, same, variant);
+  if (multi) {
+    const int v = variant >= 0 && variant < kPipeVariants ? variant : 0;
+    return pipe_variant_rows(v) == 4 ? pipe_info_for<4>(prec, uniform, same, v)
+                                     : pipe_info_for<8>(prec, uniform, same, v);
+  }
   switch (rows_per_lane) {
     case 1: return info_for<1, false>(prec, uniform, same, variant);
     case 2: return info_for<2, false>(prec, uniform, same, variant);

@@ -1,0 +1,352 @@
+// pairhmm_pipe.cuh -- multi-pass sweeps of long reads with the passes of one
+// work item running concurrently on the warps of a block.
+//
+// A read longer than one pass (32 lanes x R rows) is swept in passes of 32R
+// rows; pass p needs the last row of pass p-1 (its boundary row) column by
+// column.  Swept one pass after the other by one warp, a pair of a 2,000-base
+// read and a 5,000-base haplotype takes 8 x 5,031 steps in sequence, and the
+// longest pairs of a batch set the length of the whole launch.  Here the W
+// warps of a block take one work item together: warp w sweeps passes w, w+W,
+// w+2W, ...  Lane 31 of the warp on pass p writes the pass's last row into a
+// boundary row in global memory and publishes, every 32 columns, how far it
+// has come; lane 0 of the warp on pass p+1 reads that row through the
+// shared-memory ring of the single-warp sweep (cp.async, 32 columns ahead),
+// waiting for the publication before each chunk.  Pass p+1 thus trails pass p
+// by about 100 steps instead of a whole pass, and the item's sweep takes
+// about ceil(P/W) passes plus (W-1) x 100 steps.
+//
+// Boundary rows.  A block owns W+1 rows; pass p writes row p mod (W+1) and
+// reads row (p-1) mod (W+1).  The next pass to write a row, p+W+1, runs on
+// the same warp as p+1, the row's only reader, after p+1 has finished, so a
+// producer never waits for a consumer.  Every wait is a consumer (pass p)
+// waiting for its producer (pass p-1): waits point to strictly earlier passes,
+// so they cannot form a cycle.  Each wait also gives up after a bounded number
+// of polls, sets kErrWaitTimeout and stops the item, so a kernel always ends.
+//
+// Progress words live in shared memory: (pass << 17) | column, written with a
+// CTA-scope release by the producing lane after its row stores (and a block
+// fence), read with a CTA-scope acquire by every lane of the consumer before
+// it copies the chunk.  Both warps are in one block, so they share the SM's
+// L1 and the CTA scope suffices.
+//
+// FP32 items stop early as in the single-warp sweep: after each pass but the
+// last, the warp that swept it bounds the likelihood by the sum of the row it
+// wrote (Forward::row_bound_rejects); once both slots are below the acceptance
+// bound the item stops on every warp and both pairs go to FP64.  The bound is
+// exact, so the rescued pairs and every result are those of the full sweep.
+//
+// Results are committed after a block barrier at the end of the item: by the
+// warp that swept the last pass, or, for a rejected item, as FP64 rescues.
+// The per-cell arithmetic is the single-warp sweep's (Forward::cells), and the
+// pass count (pipe_passes, layout.h) leaves at least one pass-through row at
+// the end, so a result is always the column sum of a pass-through row: it
+// depends neither on W nor on the strip height R nor on the item's other read.
+#pragma once
+#include "pairhmm_fwd.cuh"
+
+namespace rodv {
+
+__device__ __forceinline__ uint32_t ld_acquire_cta(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.cta.shared.u32 %0, [%1];"
+               : "=r"(v)
+               : "r"((unsigned)__cvta_generic_to_shared(p))
+               : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_cta(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.cta.shared.u32 [%0], %1;" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(p)),
+               "r"(v)
+               : "memory");
+}
+
+template <class P, int R, bool UNIFORM, bool SAME, int MINB, int W>
+struct PipeForward {
+  using F = Forward<P, R, UNIFORM, true, SAME, MINB>;
+  using V = typename P::V;
+  using S = typename P::S;
+  using Cell = typename F::BoundaryCell;
+  static constexpr int kRows = W + 1;                   // boundary rows per block
+  static constexpr int kSmemPerWarp = F::kSmemPerWarp;  // emission table + cell ring
+  // polls of a progress word (about 100 ns each) before a wait gives up
+  static constexpr uint32_t kWaitPolls = 1u << 24;
+  static constexpr uint32_t kStopRejected = 1u, kStopFailed = 2u;
+
+  struct Ctl {
+    uint32_t item;
+    uint32_t stop;         // 0, kStopRejected or kStopFailed
+    uint32_t prog[kRows];  // per boundary row: (pass << 17) | last column published
+  };
+
+  __device__ __forceinline__ static uint32_t enc(uint32_t pass, uint32_t col) {
+    return (pass << 17) | col;
+  }
+
+  __device__ __forceinline__ static bool stopped(Ctl& ctl) {
+    return __any_sync(kFullMask, *reinterpret_cast<volatile uint32_t*>(&ctl.stop) != 0u);
+  }
+
+  // The whole warp waits until boundary row `row` is published up to `want`;
+  // false (in every lane) when the item stopped meanwhile or the wait expired.
+  __device__ static bool wait_prog(Ctl& ctl, int row, uint32_t want, uint32_t* err) {
+    for (uint32_t k = 0;; ++k) {
+      if (__all_sync(kFullMask, ld_acquire_cta(&ctl.prog[row]) >= want)) return true;
+      if (stopped(ctl)) return false;
+      if (k >= kWaitPolls) {
+        if ((threadIdx.x & (kWarp - 1)) == 0) {
+          atomicOr(err, kErrWaitTimeout);
+          atomicExch(&ctl.stop, kStopFailed);
+        }
+        __syncwarp();
+        return false;
+      }
+      __nanosleep(64);
+    }
+  }
+
+  // What the warp of the item's last pass keeps for the commit.
+  struct Sums {
+    V acc_m, acc_i;
+    S frozen_m, frozen_i;
+    uint32_t passes;
+    bool ok;  // the item's descriptors were valid
+  };
+
+  // This warp's passes of work item `item`.
+  __device__ static Sums run(const BatchView& b, const ClassLaunch& c, uint32_t item, int warp,
+                             int lane, uint4* table, Ctl& ctl, Cell* rows) {
+    Sums out;
+    out.acc_m = P::zero();
+    out.acc_i = P::zero();
+    out.frozen_m = 0;
+    out.frozen_i = 0;
+    out.passes = 0;
+    out.ok = false;
+    PairRef refs[2];
+    F::load_refs(c, item, refs);
+    SlotInfo sl[2];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const bool valid = (s == 0) || refs[1].read != kNoPair;
+      const PairRef r = valid ? refs[s] : refs[0];
+      const HapDesc hd = b.haps[r.hap];
+      const ReadDesc rd = b.reads[r.read];
+      sl[s].hap = b.hap_codes + hd.code_off;
+      sl[s].H = hd.len;
+      sl[s].L = rd.len;
+      sl[s].row_off = rd.row_off;
+    }
+    const uint32_t Lmax = sl[0].L > sl[1].L ? sl[0].L : sl[1].L;
+    if (sl[0].H == 0 || sl[1].H == 0 || sl[0].L == 0 || sl[1].L == 0 ||
+        (F::kSameHap && sl[0].hap != sl[1].hap) || sl[1].H > sl[0].H ||
+        (uint64_t)sl[0].H + 40 > c.scratch_cols) {
+      if (warp == 0 && lane == 0) atomicOr(c.error_flags, kErrBadLength);
+      return out;
+    }
+    out.ok = true;
+    const uint32_t passes = pipe_passes(Lmax, R);
+    out.passes = passes;
+    const uint32_t H = sl[0].H;
+    const int nsteps = (int)H + kWarp - 1;         // slot x has the longer haplotype
+    const int nfreeze = (int)sl[1].H + kWarp - 1;  // slot y's last accumulated step + 1
+    const V init = P::make(P::init_const() / (S)sl[0].H, P::init_const() / (S)sl[1].H);
+    const uint32_t L[2] = {sl[0].L, sl[1].L};
+    const uint64_t row_off[2] = {sl[0].row_off, sl[1].row_off};
+    Cell* ring = reinterpret_cast<Cell*>(table + F::Shape::kBytesPerWarp / 16);
+
+    for (uint32_t p = (uint32_t)warp; p < passes; p += W) {
+      if (stopped(ctl)) break;
+      const bool last = p + 1 == passes;
+      const int out_row = (int)(p % kRows);
+      const int in_row = (int)((p + kRows - 1) % kRows);
+      Cell* dst = rows + (size_t)out_row * c.scratch_cols;
+      const Cell* src = rows + (size_t)in_row * c.scratch_cols;
+      // cells of steps [32 k, 32 k + 32) from the previous pass's row
+      // (columns 32 k + 1 .. 32 k + 32), copied once they are published
+      auto fetch_chunk = [&](int k) -> bool {
+        const uint32_t first = (uint32_t)k * kWarp + 1u;
+        if (first <= H) {
+          const uint32_t upto = first + kWarp - 1 < H ? first + kWarp - 1 : H;
+          if (!wait_prog(ctl, in_row, enc(p - 1, upto), c.error_flags)) return false;
+        }
+        const uint32_t idx = first + (uint32_t)lane;
+        if (idx < c.scratch_cols) {
+          Cell* d = ring + (k & 1) * kWarp + lane;
+          const Cell* s = src + idx;
+          cp_async8(&d->m, &s->m);
+          cp_async8(&d->i, &s->i);
+          cp_async8(&d->d, &s->d);
+        }
+        cp_async_commit();
+        return true;
+      };
+
+      typename F::Priors pr;
+      F::load_rows(b, L, row_off, p * (kWarp * R) + lane * R, lane, table, pr);
+      V M[R], I[R], D[R];
+#pragma unroll
+      for (int k = 0; k < R; ++k) M[k] = I[k] = D[k] = P::zero();
+      V dg_m = P::zero(), dg_i = P::zero(), dg_d = P::zero();
+      if (lane == 0 && p == 0) dg_d = init;
+      const uint8_t* hx = sl[0].hap - lane;
+      const uint8_t* hy = sl[1].hap - lane;
+      const bool from_ring = p > 0;
+      bool alive = true;
+      if (from_ring) alive = fetch_chunk(0);
+      uint32_t cx_next = hx[0], cy_next = F::kSameHap ? 0u : (uint32_t)hy[0];
+      V acc_m = P::zero(), acc_i = P::zero();
+      S frozen_m = 0, frozen_i = 0;
+
+#pragma unroll 2
+      for (int s = 0; s < nsteps; ++s) {
+        if (!alive) break;
+        const uint32_t cx = cx_next, cy = cy_next;
+        cx_next = hx[s + 1];
+        if (!F::kSameHap) cy_next = hy[s + 1];
+        if ((s & (kWarp - 1)) == 0) {
+          if (from_ring) {
+            cp_async_wait_all();  // this chunk's cells
+            __syncwarp();
+            if (!fetch_chunk(s / kWarp + 1)) {
+              alive = false;
+              break;
+            }
+          } else if (stopped(ctl)) {
+            alive = false;
+            break;
+          }
+        }
+        V up_m = P::shfl_up(M[R - 1]);
+        V up_i = P::shfl_up(I[R - 1]);
+        V up_d = P::shfl_up(D[R - 1]);
+        if (lane == 0) {
+          if (from_ring) {
+            const Cell cell = ring[((s / kWarp) & 1) * kWarp + (s & (kWarp - 1))];
+            up_m = cell.m; up_i = cell.i; up_d = cell.d;
+          } else {
+            up_m = P::zero(); up_i = P::zero(); up_d = init;
+          }
+        }
+        V e[R], t_last;
+        F::load_emission(table, lane, cx, cy, e);
+        F::cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr, t_last);
+        if (!last && lane == kWarp - 1) {
+          const int col = s - (kWarp - 1) + 1;
+          if (col >= 1 && col <= (int)H) {
+            Cell cell;
+            cell.m = M[R - 1]; cell.i = I[R - 1]; cell.d = D[R - 1];
+            dst[col] = cell;
+            if ((col & (kWarp - 1)) == 0 || col == (int)H) {
+              __threadfence_block();
+              st_release_cta(&ctl.prog[out_row], enc(p, (uint32_t)col));
+            }
+          }
+        }
+        if (last) {
+          acc_m = P::fma(t_last, e[R - 1], acc_m);  // += M[R-1], one rounding
+          acc_i = P::add(acc_i, I[R - 1]);
+          if (P::kSlots == 2 && !F::kSameHap && s == nfreeze - 1) {
+            frozen_m = P::sy(acc_m);
+            frozen_i = P::sy(acc_i);
+          }
+        }
+      }
+      if (from_ring) {
+        cp_async_wait_all();  // the prefetch past the last step lands before the ring is reused
+        __syncwarp();
+      }
+      if (!alive) break;
+      if (last) {
+        out.acc_m = acc_m;
+        out.acc_i = acc_i;
+        out.frozen_m = frozen_m;
+        out.frozen_i = frozen_i;
+      } else if constexpr (P::kSlots == 2) {
+        __syncwarp();  // lane 31's row stores are visible to the whole warp
+        const uint32_t Hs[2] = {sl[0].H, sl[1].H};
+        if (F::row_bound_rejects(b, c, dst, Hs, L, (p + 1) * (kWarp * R) - 1, lane, item)) {
+          if (lane == 0) atomicCAS(&ctl.stop, 0u, kStopRejected);
+          break;
+        }
+      }
+    }
+    return out;
+  }
+
+  // After the block barrier that ends the item: the results, or the FP64
+  // rescue of a rejected item.
+  __device__ static void commit(const BatchView& b, const ClassLaunch& c, uint32_t item,
+                                int warp, int lane, const Ctl& ctl, const Sums& sm) {
+    if (!sm.ok) return;
+    const uint32_t stop = ctl.stop;
+    if (stop == kStopFailed) return;  // the error flag is set
+    PairRef fr[2];
+    F::load_refs(c, item, fr);
+    const bool valid_y = P::kSlots == 2 && fr[1].read != kNoPair;
+    if (stop == kStopRejected) {
+      if (warp == 0 && lane == 0) {
+        F::finish(b, c, fr[0], 0.0);
+        if (valid_y) F::finish(b, c, fr[1], 0.0);
+      }
+      return;
+    }
+    if (warp != (int)((sm.passes - 1) % W) || lane != kWarp - 1) return;
+    S fm = sm.frozen_m, fi = sm.frozen_i;
+    if (P::kSlots == 2 && F::kSameHap) {  // both slots ran exactly their own columns
+      fm = P::sy(sm.acc_m);
+      fi = P::sy(sm.acc_i);
+    }
+    const uint32_t Lx = b.reads[fr[0].read].len;
+    const uint32_t Ly = valid_y ? b.reads[fr[1].read].len : 0u;
+    const uint32_t rows = sm.passes * kWarp * R;
+    double res[2] = {0.0, 0.0};
+    double amin[2] = {(double)kMinAcceptedF, (double)kMinAcceptedF};
+    if (F::kScaled) {
+      res[0] = F::scaled_result(b, fr[0].read, Lx, rows, P::sx(sm.acc_m), P::sx(sm.acc_i),
+                                &amin[0]);
+      if (valid_y) res[1] = F::scaled_result(b, fr[1].read, Ly, rows, fm, fi, &amin[1]);
+    } else if (UNIFORM) {
+      res[0] = F::uniform_gapm(b, fr[0].read) * P::sx(sm.acc_m) + P::sx(sm.acc_i);
+      if (valid_y) res[1] = F::uniform_gapm(b, fr[1].read) * fm + fi;
+    } else {
+      res[0] = P::sx(sm.acc_m) + P::sx(sm.acc_i);
+      res[1] = fm + fi;
+    }
+    F::finish(b, c, fr[0], res[0], amin[0]);
+    if (valid_y) F::finish(b, c, fr[1], res[1], amin[1]);
+  }
+};
+
+// One work item per block at a time; c.scratch holds kRows boundary rows of
+// c.scratch_cols cells for every block of the grid.
+template <class P, int R, bool UNIFORM, bool SAME, int MINB, int W>
+__global__ void __launch_bounds__(W * kWarp, MINB)
+    forward_pipe_kernel(BatchView b, ClassLaunch c) {
+  using F = PipeForward<P, R, UNIFORM, SAME, MINB, W>;
+  extern __shared__ uint4 smem[];
+  __shared__ typename F::Ctl ctl;
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int warp = threadIdx.x / kWarp;
+  uint4* table = smem + warp * (F::kSmemPerWarp / 16);
+  typename F::Cell* rows = reinterpret_cast<typename F::Cell*>(c.scratch) +
+                           (size_t)blockIdx.x * F::kRows * c.scratch_cols;
+  const uint32_t n = c.work_count ? *c.work_count : c.static_count;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      ctl.item = atomicAdd(c.counter, 1u);
+      ctl.stop = 0;
+#pragma unroll
+      for (int k = 0; k < F::kRows; ++k) ctl.prog[k] = 0;
+    }
+    __syncthreads();
+    const uint32_t item = ctl.item;
+    if (item >= n) break;
+    const typename F::Sums sm = F::run(b, c, item, warp, lane, table, ctl, rows);
+    __syncthreads();
+    F::commit(b, c, item, warp, lane, ctl, sm);
+    __syncthreads();  // ctl is reset for the next item
+  }
+}
+
+}  // namespace rodv

@@ -2,6 +2,7 @@
 // regions over three device batch slots (see service.h).
 #include "service.h"
 #include "trace.h"
+#include "worker_pool.h"
 
 #include <algorithm>
 #include <cmath>
@@ -112,8 +113,9 @@ uint64_t Service::estimate_bytes(const rodv_batch& b, uint64_t pairs) const {
   }
   bytes += (uint64_t)(b.num_haps + b.num_reads) * 16;
   bytes += pairs * (16 + 12 + 8);
-  // boundary scratch: 24 bytes per column per resident warp of a multi-pass kernel
-  if (multi) bytes += (uint64_t)engine_.num_sms_ * 8 * 4 * (max_h + 40) * 24;
+  // boundary scratch: 24 bytes per column per boundary row of the multi-pass
+  // kernels, one region per multi-pass class
+  if (multi) bytes += 2 * (uint64_t)engine_.multi_scratch_rows() * (max_h + 40) * 24 + 512;
   return bytes;
 }
 
@@ -252,35 +254,54 @@ void Service::worker() {
 rodv_status Service::launch(Slot& s) {
   TraceRange trace("rodv service: form and launch batch");
   const Clock::time_point t0 = Clock::now();
-  // the combined batch: requests' regions, haplotypes and reads back to back
-  s.regions.clear();
-  s.hap_bases.clear();
-  s.read_bases.clear();
-  for (auto& q : s.quals) q.clear();
-  s.hap_off.clear();
-  s.read_off.clear();
-  s.hap_len.clear();
-  s.read_len.clear();
+  // The combined batch: requests' regions, haplotypes and reads back to back,
+  // in the slot's arrays (resized below; every element is overwritten).
+  // Each request's arrays go to offsets known in advance, so the copies run
+  // on the worker pool (one serial copy of every batch's bases and qualities
+  // took a large share of the worker's time at saturation).
+  struct Off {
+    uint64_t reg, hap, read, hb, rb;
+  };
+  std::vector<Off> offs(s.reqs.size() + 1);
   uint64_t est = 0;
-  for (const auto& r : s.reqs) {
+  for (size_t k = 0; k < s.reqs.size(); ++k) {
+    const auto& r = s.reqs[k];
     r->started = t0;
     est += r->bytes;
-    const uint32_t h0 = (uint32_t)s.hap_len.size(), r0 = (uint32_t)s.read_len.size();
-    const uint64_t hb0 = s.hap_bases.size(), rb0 = s.read_bases.size();
-    for (rodv_region rg : r->regions) {
-      rg.hap_start += h0;
-      rg.read_start += r0;
-      s.regions.push_back(rg);
-    }
-    s.hap_bases.insert(s.hap_bases.end(), r->hap_bases.begin(), r->hap_bases.end());
-    s.read_bases.insert(s.read_bases.end(), r->read_bases.begin(), r->read_bases.end());
-    for (int q = 0; q < 4; ++q)
-      s.quals[q].insert(s.quals[q].end(), r->quals[q].begin(), r->quals[q].end());
-    for (uint64_t o : r->hap_off) s.hap_off.push_back(o + hb0);
-    for (uint64_t o : r->read_off) s.read_off.push_back(o + rb0);
-    s.hap_len.insert(s.hap_len.end(), r->hap_len.begin(), r->hap_len.end());
-    s.read_len.insert(s.read_len.end(), r->read_len.begin(), r->read_len.end());
+    offs[k + 1] = Off{offs[k].reg + r->regions.size(), offs[k].hap + r->hap_len.size(),
+                      offs[k].read + r->read_len.size(), offs[k].hb + r->hap_bases.size(),
+                      offs[k].rb + r->read_bases.size()};
   }
+  const Off& tot = offs.back();
+  s.regions.resize(tot.reg);
+  s.hap_bases.resize(tot.hb);
+  s.read_bases.resize(tot.rb);
+  for (auto& q : s.quals) q.resize(tot.rb);
+  s.hap_off.resize(tot.hap);
+  s.read_off.resize(tot.read);
+  s.hap_len.resize(tot.hap);
+  s.read_len.resize(tot.read);
+  parallel_for(s.reqs.size(), 1, [&](size_t lo, size_t hi) {
+    for (size_t k = lo; k < hi; ++k) {
+      const Request& r = *s.reqs[k];
+      const Off& o = offs[k];
+      for (size_t g = 0; g < r.regions.size(); ++g) {
+        rodv_region rg = r.regions[g];
+        rg.hap_start += (uint32_t)o.hap;
+        rg.read_start += (uint32_t)o.read;
+        s.regions[o.reg + g] = rg;
+      }
+      std::memcpy(s.hap_bases.data() + o.hb, r.hap_bases.data(), r.hap_bases.size());
+      std::memcpy(s.read_bases.data() + o.rb, r.read_bases.data(), r.read_bases.size());
+      for (int q = 0; q < 4; ++q)
+        std::memcpy(s.quals[q].data() + o.rb, r.quals[q].data(), r.quals[q].size());
+      for (size_t h = 0; h < r.hap_off.size(); ++h) s.hap_off[o.hap + h] = r.hap_off[h] + o.hb;
+      for (size_t j = 0; j < r.read_off.size(); ++j)
+        s.read_off[o.read + j] = r.read_off[j] + o.rb;
+      std::memcpy(s.hap_len.data() + o.hap, r.hap_len.data(), r.hap_len.size() * 4);
+      std::memcpy(s.read_len.data() + o.read, r.read_len.data(), r.read_len.size() * 4);
+    }
+  });
   const Clock::time_point t_comb = Clock::now();
   const rodv_batch b{(uint32_t)s.regions.size(), s.regions.data(), (uint32_t)s.hap_len.size(),
                      s.hap_bases.data(), s.hap_off.data(), s.hap_len.data(),

@@ -197,6 +197,103 @@ def test_long_pairs_multi_pass(engine):
     assert np.abs(got[finite] - ref[finite]).max() < TOL
 
 
+def test_long_pairs_c3_sample_against_reference(engine):
+    """64 pairs of the long-pair configuration (1-2 kb reads x 2-5 kb
+    haplotypes, 5% substitutions, 1% indels: every pair goes to FP64) against
+    the reference's own schedule_pairhmm output and the FP64 oracle."""
+    b = workloads.make_workload("long", scale=0.032)
+    assert b.num_pairs == 64
+    got, st = engine.batch(b, stats=True)
+    assert np.abs(got - oracle.batch_log10(b, oracle.REFERENCE)).max() < TOL
+    if oracle.ref_available():
+        ref = oracle.ref_schedule(b)
+        fin = np.isfinite(ref)
+        assert np.array_equal(fin, np.isfinite(got))
+        assert np.abs(got[fin] - ref[fin]).max() < TOL
+    assert st["fp64_pairs"] == b.num_pairs
+
+
+def _long_mixed_batch(seed=21):
+    """Long reads of both multi-pass classes (uniform and per-row gap
+    qualities), one to three reads per region (same-haplotype items and
+    two-haplotype leftovers), lengths around the pass boundaries of both
+    strip heights (128 and 256 rows), some pairs below the FP32 bound."""
+    rng = np.random.default_rng(seed)
+    regs = []
+    lengths = [257, 300, 383, 384, 385, 511, 512, 513, 640, 767, 768, 1100]
+    for k, L in enumerate(lengths):
+        hl = L + int(rng.integers(40, 400))
+        hap = workloads._random_seq(rng, hl)
+        reads, qs, ins, dele, gcp = [], [], [], [], []
+        for j in range(1 + k % 3):
+            st = int(rng.integers(0, hl - L + 1))
+            rd = workloads._mutate(rng, hap[st:st + L], 0.06 if (k + j) % 4 == 0 else 0.005, 0.0)
+            n = len(rd)
+            reads.append(rd)
+            qs.append(workloads._quals(rng, n, 20, 40))
+            if k % 2:
+                ins.append(workloads._quals(rng, n, 30, 45))
+                dele.append(workloads._quals(rng, n, 30, 45))
+                gcp.append(workloads._quals(rng, n, 5, 15))
+            else:
+                ins.append(np.full(n, 45, np.uint8))
+                dele.append(np.full(n, 45, np.uint8))
+                gcp.append(np.full(n, 10, np.uint8))
+        hap2 = workloads._mutate(rng, hap, 0.01, 0.001)
+        regs.append(([hap, hap2], reads, qs, ins, dele, gcp))
+    return Batch.from_regions(regs)
+
+
+def _engine_with_multi_variants(tmp_path, v32, v64, force_fp64=False):
+    """An engine whose two multi-pass classes use FP32 variant v32 and FP64
+    variant v64 (from a tuning cache written for it); single-pass classes
+    keep the tuned choice."""
+    from rodv_b200 import Engine
+    base = tmp_path / "tuned.txt"
+    if not base.exists():
+        e = Engine(0)
+        e.autotune(str(base))
+        e.close()
+    lines = []
+    for ln in base.read_text().splitlines():
+        key, c, v, w = ln.split()
+        if int(c) >= 16:
+            v, w = str(v32), str(v64)
+        lines.append(" ".join((key, c, v, w)))
+    path = tmp_path / f"multi_{v32}_{v64}.txt"
+    path.write_text("\n".join(lines) + "\n")
+    e = Engine(0, autotune=1, tune_cache=str(path), force_fp64=force_fp64)
+    tv = e.tuned_variants()
+    assert tv["fp32"][16:] == [v32, v32] and tv["fp64"][16:] == [v64, v64]
+    return e
+
+
+def test_multi_pass_variants_give_identical_results(tmp_path):
+    """Every strip height (4 or 8 rows per lane) and every number of warps
+    sweeping one item's passes (2 or 4) gives bitwise the same results, FP32
+    with rescue and forced FP64 alike, and they match the oracle."""
+    b = _long_mixed_batch()
+    ref = oracle.batch_log10(b)
+    ref64 = oracle.batch_log10(b, oracle.FP64)
+    first32 = first64 = None
+    for v in range(4):
+        e = _engine_with_multi_variants(tmp_path, v, v)
+        got, st = e.batch(b, stats=True)
+        e.close()
+        assert 0 < st["fp64_pairs"] < b.num_pairs
+        assert np.abs(got - ref).max() < TOL, v
+        if first32 is None:
+            first32 = got
+        assert np.array_equal(got, first32), v
+        e = _engine_with_multi_variants(tmp_path, v, v, force_fp64=True)
+        got64 = e.batch(b)
+        e.close()
+        assert np.abs(got64 - ref64).max() < 1e-9, v
+        if first64 is None:
+            first64 = got64
+        assert np.array_equal(got64, first64), v
+
+
 def test_multi_pass_fp32_path():
     """Reads longer than one pass that stay in FP32 range (high identity)."""
     from rodv_b200 import Engine
