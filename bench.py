@@ -39,6 +39,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -49,19 +50,56 @@ sys.path.insert(0, ROOT)
 METRIC = ("PairHMM GCUPS on 1 B200 (batched vs plain GPU form, % FP32 peak) vs host AVX; "
           "p99 ms")
 FLOPS_PER_CELL = 12
-TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "forward_kernels_dram_traffic_uneven_full.md")
+# every result must be within this many log10 units of the FP64 oracle and of
+# the reference's own output
+ACCURACY_TOL = 1e-3
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "forward_kernel_dram_traffic_uneven.md")
+# The device sources whose compiled code the traffic capture measured.
+KERNEL_SOURCES = ["pairhmm_fwd.cuh", "pairhmm_pipe.cuh", "layout.h", "kernel_table.cuh",
+                  "kernels.h", "pairhmm_kernels.cu", "kernels_r*.cu", "kernels_multi_r*.cu"]
+
+
+def kernel_source_sha():
+    """sha256 (first 16 hex digits) of the forward kernels' sources."""
+    import glob
+    import hashlib
+    h = hashlib.sha256()
+    csrc = os.path.join(ROOT, "rodv_b200", "csrc")
+    names = sorted({os.path.basename(p) for pat in KERNEL_SOURCES
+                    for p in glob.glob(os.path.join(csrc, pat))})
+    for name in names:
+        with open(os.path.join(csrc, name), "rb") as fh:
+            h.update(name.encode() + b"\0" + fh.read())
+    return h.hexdigest()[:16]
+
+
+def profile_fields(path=TRAFFIC_PROFILE):
+    """The `key: value` lines of an ncu summary."""
+    out = {}
+    if os.path.exists(path):
+        with open(path) as fh:
+            for ln in fh:
+                if ":" in ln and not ln.startswith(("#", "|", " ", "`", "*")):
+                    k, v = ln.split(":", 1)
+                    out[k.strip()] = v.strip()
+    return out
 
 
 def step_traffic_bytes(workload, scale):
-    """DRAM bytes (read + write) of the FP32 kernels of one resident step, from the ncu
-    capture summarised in TRAFFIC_PROFILE; None for any other workload or size."""
-    if workload != "uneven" or scale != 1.0 or not os.path.exists(TRAFFIC_PROFILE):
-        return None
-    with open(TRAFFIC_PROFILE) as fh:
-        for ln in fh:
-            if ln.startswith("fp32_step_traffic_bytes:"):
-                return int(ln.split(":")[1])
-    return None
+    """DRAM bytes (read + write) of the FP32 kernels of one resident step of the
+    full-size uneven workload: the capture of the dominant class's kernel in
+    TRAFFIC_PROFILE, scaled to the step by that class's share of the step's
+    cells.  Returns (bytes or None, note).  A capture taken on other kernel
+    sources than these is not reported (the note says so)."""
+    if workload != "uneven" or scale != 1.0:
+        return None, "captured for the full-size uneven workload only"
+    f = profile_fields()
+    if "fp32_step_traffic_bytes" not in f:
+        return None, f"no traffic capture in {os.path.relpath(TRAFFIC_PROFILE, ROOT)}"
+    if f.get("kernel_source_sha16") != kernel_source_sha():
+        return None, ("STALE: the traffic capture measured kernel sources "
+                      f"{f.get('kernel_source_sha16')}, this build has {kernel_source_sha()}")
+    return int(f["fp32_step_traffic_bytes"]), f.get("traffic_note", "")
 
 
 def log(*a):
@@ -81,10 +119,11 @@ class Clocks:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, path: str = ""):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{gpu_index}.csv")
+        self.path = path or os.path.join(tempfile.gettempdir(),
+                                         f"rodv_clocks_gpu{gpu_index}_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
@@ -237,7 +276,8 @@ def run_engine(args, world, rank, local):
             f"{cells:.3e} cells (generated in {time.perf_counter() - t_gen:.1f} s)")
     eng = Engine(local)
     t_tune = time.perf_counter()
-    variants = eng.autotune()
+    eng.autotune()
+    variants = eng.tuned_variants()
     t_tune = time.perf_counter() - t_tune
     peaks = eng.measure_peaks()
     db = eng.upload(batch)
@@ -247,7 +287,7 @@ def run_engine(args, world, rank, local):
         db.run()
     barrier()
     dev_ms, fp32_ms, step_ms, launches, fp64_pairs = [], [], [], 0, 0
-    with Clocks(local) as clk:
+    with Clocks(local, args.clocks_out) as clk:
         t0 = time.perf_counter()
         for _ in range(args.steps):
             ts = time.perf_counter()
@@ -273,7 +313,7 @@ def run_engine(args, world, rank, local):
         eng.batch_into(holder, out)
     barrier()
     e2e_ms, h2d, d2h = [], 0, 0
-    for _ in range(args.e2e_steps):
+    for _ in range(args.e2e_steps or args.steps):
         t = time.perf_counter()
         st = eng.batch_into(holder, out)
         e2e_ms.append((time.perf_counter() - t) * 1e3)
@@ -293,7 +333,9 @@ def run_engine(args, world, rank, local):
         configs = config_lines(eng, args, value) if not args.no_configs else None
         cpu = None
         if not args.no_cpu_baseline:
-            cpu = cpu_baseline(args, eng)
+            cpu = cpu_baseline(args)
+        accuracy = accuracy_per_config(eng) if not args.no_accuracy else None
+        traffic, traffic_note = step_traffic_bytes(args.workload, args.scale)
         stream = streaming_c5(args) if args.stream_requests > 0 else None
         line = {
             "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world,
@@ -306,17 +348,21 @@ def run_engine(args, world, rank, local):
                        "l2": "inputs larger than L2 (resident batch ~%.2f GB)" %
                              (batch.input_bytes() / 1e9),
                        "parallelism": f"dp{world} (regions sharded, no collective)",
-                       "tuned_variants": variants, "tune_s": round(t_tune, 2)},
+                       "tuned_variants_fp32": variants["fp32"],
+                       "tuned_variants_fp64": variants["fp64"], "tune_s": round(t_tune, 2)},
             "e2e": {"value": e2e_value, "unit": "GCUPS", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "steps": len(e2e_ms),
                     "ms_per_step": e2e_total / len(e2e_ms) * 1e3,
                     "max_abs_diff_vs_resident_run": same},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": achieved / peak,
-                         "traffic": step_traffic_bytes(args.workload, args.scale),
+                         "traffic": traffic,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
-                                           "of the FP32 kernels of one step (" +
-                                           os.path.relpath(TRAFFIC_PROFILE, ROOT) + ")",
+                                           "of the dominant FP32 class kernel, scaled to one "
+                                           "step by its cell share (" +
+                                           os.path.relpath(TRAFFIC_PROFILE, ROOT) + "); " +
+                                           traffic_note,
+                         "kernel_source_sha16": kernel_source_sha(),
                          "kernel": "forward_kernel<F32x2,...> (all FP32 classes of a step)",
                          "flops_per_cell": FLOPS_PER_CELL,
                          "peak_source": "FFMA-chain kernel measured in this run "
@@ -336,10 +382,26 @@ def run_engine(args, world, rank, local):
         }
         if plain:
             line["plain_form"] = plain
+            line["config"]["C1_plain_speedup"] = plain["speedup"]
         if cpu:
             line["cpu_baseline"] = cpu
         if configs:
-            line["configs"] = configs
+            line["configs"] = {k: v for c in configs for k, v in flat_config(c).items()}
+            for c in configs:
+                if c["config"] in ("C1", "C3", "C4", "C5"):
+                    line["config"][c["config"] + "_gcups"] = c["gcups"]
+        if accuracy:
+            line["accuracy"] = {k: v for a in accuracy for k, v in flat_accuracy(a).items()}
+            worst = []
+            for key in ("vs_fp64_oracle", "vs_reference"):
+                vals = [a[key]["max"] for a in accuracy if a[key]["max"] is not None]
+                line["config"]["max_abs_dlog10_" + key] = max(vals) if vals else None
+                worst += vals
+            mism = sum(a[k]["non_finite_mismatches"] for a in accuracy
+                       for k in ("vs_fp64_oracle", "vs_reference"))
+            line["accuracy"]["tolerance_log10"] = ACCURACY_TOL
+            line["accuracy"]["within_tolerance"] = bool(worst and max(worst) <= ACCURACY_TOL
+                                                        and mism == 0)
         if stream:
             line["streaming"] = stream
         print(json.dumps(line), flush=True)
@@ -596,7 +658,23 @@ def accuracy_per_config(eng):
     return out
 
 
-def cpu_baseline(args, eng=None):
+def flat_config(c):
+    """One configuration line as scalar keys prefixed by its name."""
+    name = c["config"].replace(" ", "")
+    return {f"{name}_{k}": v for k, v in c.items()
+            if k != "config" and isinstance(v, (int, float, str))}
+
+
+def flat_accuracy(a):
+    """One configuration's accuracy as scalar keys: <config>_<vs>_<stat>."""
+    out = {}
+    for key, short in (("vs_fp64_oracle", "oracle"), ("vs_reference", "reference")):
+        for stat in ("max", "mean", "pairs", "non_finite_mismatches"):
+            out[f"{a['config']}_{short}_{stat}"] = a[key][stat]
+    return out
+
+
+def cpu_baseline(args):
     import oracle
     if not oracle.ref_available():
         return {"value": None, "unit": "GCUPS", "cores": 0, "kind": "reference",
@@ -609,8 +687,6 @@ def cpu_baseline(args, eng=None):
                      f"{batch.cells():.3e} cells of the {args.workload} workload, "
                      f"{dt:.1f} s on {threads} threads",
            "cpu": cpu_model()}
-    if eng is not None:
-        res["accuracy_per_config"] = accuracy_per_config(eng)
     return res
 
 
@@ -625,9 +701,14 @@ def main():
                          "service measurement only")
     ap.add_argument("--workload", default="uneven")
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=0,
+                    help="timed calls of the e2e measurement (0: the same as --steps)")
+    ap.add_argument("--clocks-out", default="",
+                    help="CSV of the nvidia-smi clock samples (default: a temporary file)")
     ap.add_argument("--plain-pairs", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the per-configuration accuracy samples")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the per-configuration throughput lines (C1, C3-C5)")
     ap.add_argument("--tune", action="store_true", help="profile mode: autotune first")
