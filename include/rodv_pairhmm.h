@@ -19,6 +19,12 @@
  *   pairhmm::inter::compute_inter_pairhmm_{AVX2,AVX512}_{float,double}
  *                                           src/core/pairhmm/inter/pairhmm_inter_api.h:17-24
  *       -> rodv_pairhmm_batch with one single-pair region per test case
+ *          (islog10 = true), rodv_pairhmm_batch_raw (islog10 = false)
+ * Base comparison: the engine applies the intra kernel's rule everywhere
+ * ('N' on either side matches any base, pairhmm_impl.cpp:26-42), also where
+ * roDV's inter kernel compares raw bytes (inter/simd_traits_avx2.h:61-63);
+ * roDV's scheduler never sends a pair with 'N' to the inter kernel, so the
+ * two agree on every pair schedule_pairhmm computes.
  */
 #ifndef RODV_PAIRHMM_H_
 #define RODV_PAIRHMM_H_
@@ -131,6 +137,21 @@ void rodv_engine_destroy(rodv_engine* engine);
  * FP32 with FP64 rescue below 1e-28.  stats may be null. */
 rodv_status rodv_pairhmm_batch(rodv_engine* engine, const rodv_batch* batch, int32_t use_double,
                                double* out_log10, rodv_stats* stats);
+
+/* The same computation returning raw likelihoods instead of log10, as
+ * compute_inter_pairhmm_*(..., islog10 = false) does
+ * (pairhmm_inter_api.h:17-24, pairhmm_schedule.cpp:229-248): out_raw[i] is
+ * the pair's scaled likelihood sum(M + I) of the last row and
+ * out_precision[i] the precision that produced it: 0 = FP32 with row 0 at
+ * 2^120/haplen (log10 = log10(raw) - 36.1236000061f; raw >= 1e-28 always),
+ * 1 = FP64 with row 0 at 2^1020/haplen (log10 = log10(raw) -
+ * 307.050595577260822; 0 where the reference's flush-to-zero gives -inf).
+ * FP32 results below the acceptance bound are recomputed in FP64 as in
+ * rodv_pairhmm_batch; use_double != 0 makes every result FP64.  Both arrays
+ * hold rodv_batch_num_pairs(batch) entries. */
+rodv_status rodv_pairhmm_batch_raw(rodv_engine* engine, const rodv_batch* batch,
+                                   int32_t use_double, double* out_raw, uint8_t* out_precision,
+                                   rodv_stats* stats);
 
 /* Number of results of a batch (sum of num_haps*num_reads). */
 uint64_t rodv_batch_num_pairs(const rodv_batch* batch);

@@ -143,6 +143,18 @@ class Engine:
                                                 _ptr(out, _lib._f64p), ctypes.byref(st)))
         return (out, st.as_dict()) if stats else out
 
+    def batch_raw(self, b: Batch, use_double: bool = False):
+        """Raw scaled likelihoods and the precision of each (0: FP32 at 2^120,
+        1: FP64 at 2^1020) -- roDV's inter API with islog10 = false."""
+        holder = _CBatchHolder(b)
+        out = np.empty(b.num_pairs, dtype=np.float64)
+        prec = np.empty(b.num_pairs, dtype=np.uint8)
+        st = _lib.Stats()
+        self._check(self.lib.rodv_pairhmm_batch_raw(self.h, ctypes.byref(holder.c),
+                                                    int(use_double), _ptr(out, _lib._f64p),
+                                                    _ptr(prec, _lib._u8p), ctypes.byref(st)))
+        return out, prec
+
     def batch_into(self, holder: _CBatchHolder, out: np.ndarray, use_double: bool = False) -> dict:
         """Like :meth:`batch` with a prepared struct and output (no allocation)."""
         st = _lib.Stats()

@@ -102,6 +102,9 @@ SIGNATURES = [
     ("rodv_engine_destroy", None, [ctypes.c_void_p]),
     ("rodv_pairhmm_batch", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(CBatch),
                                             ctypes.c_int32, _f64p, ctypes.POINTER(Stats)]),
+    ("rodv_pairhmm_batch_raw", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(CBatch),
+                                                ctypes.c_int32, _f64p, _u8p,
+                                                ctypes.POINTER(Stats)]),
     ("rodv_batch_num_pairs", ctypes.c_uint64, [ctypes.POINTER(CBatch)]),
     ("rodv_batch_validate", ctypes.c_int32, [ctypes.POINTER(CBatch), ctypes.c_char_p,
                                              ctypes.c_size_t]),

@@ -101,6 +101,15 @@ rodv_status rodv_pairhmm_batch(rodv_engine* engine, const rodv_batch* batch, int
   return engine->impl->run_host(*batch, out, stats, use_double != 0);
 }
 
+rodv_status rodv_pairhmm_batch_raw(rodv_engine* engine, const rodv_batch* batch,
+                                   int32_t use_double, double* out_raw, uint8_t* out_precision,
+                                   rodv_stats* stats) {
+  if (!engine || !batch || !out_raw || !out_precision) return RODV_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(engine->impl->mutex());
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  return engine->impl->run_host(*batch, out_raw, stats, use_double != 0, out_precision);
+}
+
 rodv_status rodv_pairhmm_pair(rodv_engine* engine, const uint8_t* hap, uint32_t hap_len,
                               const uint8_t* read, const uint8_t* q, const uint8_t* ins,
                               const uint8_t* del, const uint8_t* gcp, uint32_t read_len,

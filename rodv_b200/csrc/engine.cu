@@ -95,6 +95,7 @@ ArenaView arena_view(const PackedPlan& p, uint8_t* base, const PriorTables& tab)
   a.view.haps = reinterpret_cast<const HapDesc*>(base + p.off_haps);
   a.view.reads = reinterpret_cast<const ReadDesc*>(base + p.off_reads);
   a.view.out = reinterpret_cast<double*>(base + p.off_out);
+  a.view.raw_prec = p.raw ? base + p.off_prec : nullptr;
   a.view.tab = tab;
   a.counts = reinterpret_cast<uint32_t*>(base + p.off_counts);
   a.scratch = p.scratch_bytes ? reinterpret_cast<float*>(base + p.off_scratch) : nullptr;
@@ -389,11 +390,13 @@ rodv_status validate_batch(const rodv_batch& b, bool check_bases, uint64_t* num_
   return RODV_OK;
 }
 
-rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64) {
+rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64,
+                         bool raw) {
   TraceRange trace("rodv: pack");
   PackTimer timer(opt_.verbose >= 2);
   plan = PackedPlan{};
   plan.fp64 = fp64;
+  plan.raw = raw;
   uint64_t pairs = 0;
   {
     std::string msg;
@@ -655,6 +658,8 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   plan.upload_bytes = fp64 ? o : lists_begin;
   plan.off_out = o; o = align_up(o + pairs * 8);
   plan.off_counts = o; o = align_up(o + kCountWords * 4);
+  plan.off_prec = o;
+  if (raw) o = align_up(o + pairs);
   plan.scratch_cols = plan.multi_max_hap ? plan.multi_max_hap + 40 : 0;
   plan.off_scratch = o;
   if (plan.scratch_cols) {
@@ -982,7 +987,8 @@ double env_cells(const char* name, double fallback) {
   return x > 0 ? x : fallback;
 }
 
-rodv_status Engine::run_host(const rodv_batch& b, double* out, rodv_stats* st, bool force_fp64) {
+rodv_status Engine::run_host(const rodv_batch& b, double* out, rodv_stats* st, bool force_fp64,
+                             uint8_t* prec) {
   if (!out) return fail(RODV_ERR_INVALID_ARG, "null output");
   RODV_CUDA(cudaSetDevice(device_));
   const bool fp64 = force_fp64 || opt_.force_fp64 != 0;
@@ -1002,7 +1008,7 @@ rodv_status Engine::run_host(const rodv_batch& b, double* out, rodv_stats* st, b
   }
   static const double chunk_cells = env_cells("RODV_CHUNK_CELLS", kChunkCells);
   static const double first_cells = env_cells("RODV_FIRST_CHUNK_CELLS", kFirstChunkCells);
-  if (cum[G] < kMinChunkedCells || G < 4) return run_host_single(b, out, st, fp64);
+  if (cum[G] < kMinChunkedCells || G < 4) return run_host_single(b, out, st, fp64, prec);
   std::vector<uint32_t> bounds{0};
   double target = std::min(chunk_cells, std::max(first_cells, cum[G] / 32));
   for (uint32_t g = 1; g < G; ++g) {
@@ -1012,11 +1018,11 @@ rodv_status Engine::run_host(const rodv_batch& b, double* out, rodv_stats* st, b
     }
   }
   bounds.push_back(G);
-  if (bounds.size() < 3) return run_host_single(b, out, st, fp64);
-  return run_host_chunked(b, out, st, fp64, bounds);
+  if (bounds.size() < 3) return run_host_single(b, out, st, fp64, prec);
+  return run_host_chunked(b, out, st, fp64, bounds, prec);
 }
 
-rodv_status Engine::finish_lane(HostLane& l, double* out, rodv_stats* st) {
+rodv_status Engine::finish_lane(HostLane& l, double* out, rodv_stats* st, uint8_t* prec) {
   TraceRange trace("rodv: finish range");
   l.busy = false;
   RODV_CUDA(cudaEventSynchronize(l.done));
@@ -1035,8 +1041,10 @@ rodv_status Engine::finish_lane(HostLane& l, double* out, rodv_stats* st) {
                 "kernel reported error flags " + std::to_string(counts[kCtrError]));
   // results into the caller's (pageable) buffer, 128K pairs per task: the
   // last range's copy is on the call's critical path
+  const uint8_t* hp = h + p.num_pairs * 8 + kCountWords * 4;  // raw mode: precisions
   parallel_for(p.num_pairs, 1u << 17, [&](size_t lo, size_t hi) {
     std::memcpy(out + l.out_off + lo, h + lo * 8, (hi - lo) * 8);
+    if (prec) std::memcpy(prec + l.out_off + lo, hp + lo, hi - lo);
   });
   if (st) {
     float ms = 0.f;
@@ -1057,7 +1065,8 @@ rodv_status Engine::finish_lane(HostLane& l, double* out, rodv_stats* st) {
 }
 
 rodv_status Engine::run_host_chunked(const rodv_batch& b, double* out, rodv_stats* st,
-                                     bool fp64, const std::vector<uint32_t>& bounds) {
+                                     bool fp64, const std::vector<uint32_t>& bounds,
+                                     uint8_t* prec) {
   const auto t0 = std::chrono::steady_clock::now();
   const bool timeline = opt_.verbose >= 2;
   if (timeline) RODV_CUDA(cudaEventRecord(ev_[3], lanes_[0].stream));
@@ -1068,7 +1077,7 @@ rodv_status Engine::run_host_chunked(const rodv_batch& b, double* out, rodv_stat
   for (size_t k = 0; k < nchunks && result == RODV_OK; ++k) {
     HostLane& l = lanes_[k % kHostLanes];
     if (l.busy) {
-      result = finish_lane(l, out, &acc);
+      result = finish_lane(l, out, &acc, prec);
       if (result != RODV_OK) break;
     }
     // the range's regions over the batch's arrays, rebased to the range's
@@ -1108,7 +1117,7 @@ rodv_status Engine::run_host_chunked(const rodv_batch& b, double* out, rodv_stat
       }
     }
     const double t_pack0 = ms_since(t0);
-    result = pack(v, l.plan, l.staging, fp64);
+    result = pack(v, l.plan, l.staging, fp64, prec != nullptr);
     if (result != RODV_OK) break;
     if (timeline)
       fprintf(stderr, "rodv: range %zu (%u regions, %.2e cells): pack %.2f-%.2f ms\n", k, g1 - g0,
@@ -1116,7 +1125,7 @@ rodv_status Engine::run_host_chunked(const rodv_batch& b, double* out, rodv_stat
     const PackedPlan& p = l.plan;
     cudaError_t e = cudaSuccess;
     if (l.arena.bytes < p.total_bytes) e = l.arena.ensure(p.total_bytes + p.total_bytes / 4);
-    const size_t ob = p.num_pairs * 8 + kCountWords * 4;
+    const size_t ob = p.num_pairs * 8 + kCountWords * 4 + (p.raw ? p.num_pairs : 0);
     if (e == cudaSuccess && l.out.bytes < ob) e = l.out.ensure(ob + ob / 4);
     uint8_t* d = static_cast<uint8_t*>(l.arena.ptr);
     uint8_t* h = static_cast<uint8_t*>(l.out.ptr);
@@ -1133,6 +1142,9 @@ rodv_status Engine::run_host_chunked(const rodv_batch& b, double* out, rodv_stat
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(h + p.num_pairs * 8, d + p.off_counts, kCountWords * 4,
                           cudaMemcpyDeviceToHost, l.stream);
+    if (e == cudaSuccess && p.raw)
+      e = cudaMemcpyAsync(h + p.num_pairs * 8 + kCountWords * 4, d + p.off_prec, p.num_pairs,
+                          cudaMemcpyDeviceToHost, l.stream);
     if (e == cudaSuccess) e = cudaEventRecord(l.done, l.stream);
     if (e != cudaSuccess) {
       result = cuda_fail(e, "chunk download");
@@ -1148,7 +1160,7 @@ rodv_status Engine::run_host_chunked(const rodv_batch& b, double* out, rodv_stat
     HostLane& l = lanes_[k % kHostLanes];
     if (!l.busy) continue;
     if (result == RODV_OK) {
-      result = finish_lane(l, out, &acc);
+      result = finish_lane(l, out, &acc, prec);
     } else {
       cudaStreamSynchronize(l.stream);
       l.busy = false;
@@ -1165,13 +1177,14 @@ rodv_status Engine::run_host_chunked(const rodv_batch& b, double* out, rodv_stat
 }
 
 rodv_status Engine::run_host_single(const rodv_batch& b, double* out, rodv_stats* st,
-                                    bool fp64) {
+                                    bool fp64, uint8_t* prec) {
   const auto t0 = std::chrono::steady_clock::now();
   PackedPlan plan;
-  rodv_status s = pack(b, plan, staging_, fp64);
+  rodv_status s = pack(b, plan, staging_, fp64, prec != nullptr);
   if (s != RODV_OK) return s;
   RODV_CUDA(arena_.ensure(plan.total_bytes));
-  RODV_CUDA(out_staging_.ensure(plan.num_pairs * 8 + kCountWords * 4));
+  RODV_CUDA(out_staging_.ensure(plan.num_pairs * 8 + kCountWords * 4 +
+                                (prec ? plan.num_pairs : 0)));
   uint8_t* d = static_cast<uint8_t*>(arena_.ptr);
   RODV_CUDA(cudaEventRecord(ev_[3], stream_));
   RODV_CUDA(cudaMemcpyAsync(d, staging_.ptr, plan.upload_bytes, cudaMemcpyHostToDevice, stream_));
@@ -1182,13 +1195,18 @@ rodv_status Engine::run_host_single(const rodv_batch& b, double* out, rodv_stats
                             stream_));
   RODV_CUDA(cudaMemcpyAsync(hs + plan.num_pairs * 8, d + plan.off_counts, kCountWords * 4,
                             cudaMemcpyDeviceToHost, stream_));
+  if (prec)
+    RODV_CUDA(cudaMemcpyAsync(hs + plan.num_pairs * 8 + kCountWords * 4, d + plan.off_prec,
+                              plan.num_pairs, cudaMemcpyDeviceToHost, stream_));
   RODV_CUDA(cudaStreamSynchronize(stream_));
   const uint32_t* counts = reinterpret_cast<const uint32_t*>(hs + plan.num_pairs * 8);
   if (counts[kCtrError] != 0)
     return fail(RODV_ERR_DEVICE_CHECK,
                 "kernel reported error flags " + std::to_string(counts[kCtrError]));
+  const uint8_t* hp = hs + plan.num_pairs * 8 + kCountWords * 4;
   parallel_for(plan.num_pairs, 1u << 17, [&](size_t lo, size_t hi) {
     std::memcpy(out + lo, hs + lo * 8, (hi - lo) * 8);
+    if (prec) std::memcpy(prec + lo, hp + lo, hi - lo);
   });
   if (st) {
     fill_stats(st, plan, counts);

@@ -71,6 +71,7 @@ struct PackedPlan {
   uint32_t max_hap_len = 0;
   uint32_t multi_max_hap = 0;
   bool fp64 = false;                       // every pair computed in FP64
+  bool raw = false;                        // raw likelihoods and their precision
   // FP32 same-haplotype items: ChainItem for single-pass classes, SameItem
   // for the multi-pass ones
   uint32_t same_items[kNumClasses] = {};
@@ -86,6 +87,7 @@ struct PackedPlan {
   size_t off_preset = 0;                   // forced FP64: list lengths (uploaded)
   size_t upload_bytes = 0;                 // the H2D part starts at 0
   size_t off_out = 0, off_counts = 0, off_scratch = 0;
+  size_t off_prec = 0;                     // raw mode: precision byte per pair
   size_t total_bytes = 0;
   size_t scratch_bytes = 0;
   uint32_t scratch_cols = 0;
@@ -113,7 +115,10 @@ class Engine {
   ~Engine();
   rodv_status init();
 
-  rodv_status run_host(const rodv_batch& b, double* out, rodv_stats* st, bool force_fp64 = false);
+  // prec: null, or raw mode (rodv_pairhmm_batch_raw): out receives raw
+  // likelihoods and prec the precision of each.
+  rodv_status run_host(const rodv_batch& b, double* out, rodv_stats* st, bool force_fp64 = false,
+                       uint8_t* prec = nullptr);
   rodv_status upload(const rodv_batch& b, rodv_device_batch** out);
   rodv_status run_device(rodv_device_batch* db, rodv_stats* st);
   rodv_status download(rodv_device_batch* db, double* out);
@@ -148,7 +153,8 @@ class Engine {
   rodv_status cuda_fail(cudaError_t e, const char* where);
 
  private:
-  rodv_status pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64);
+  rodv_status pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64,
+                   bool raw = false);
   // parts: 1 = counter reset and FP32 launches, 2 = FP64 launches.  ev: null,
   // or three events recorded before the FP32 launches, between the two parts
   // and after the FP64 launches.  fan_out: each class's launches go to its own
@@ -163,10 +169,11 @@ class Engine {
   rodv_status launch_fp64_class(const PackedPlan& plan, uint8_t* dbase, int cls, int variant,
                                 cudaStream_t stream);
   rodv_status check_errors(const PackedPlan& plan, uint8_t* dbase);
-  rodv_status run_host_single(const rodv_batch& b, double* out, rodv_stats* st, bool fp64);
+  rodv_status run_host_single(const rodv_batch& b, double* out, rodv_stats* st, bool fp64,
+                              uint8_t* prec);
   rodv_status run_host_chunked(const rodv_batch& b, double* out, rodv_stats* st, bool fp64,
-                               const std::vector<uint32_t>& bounds);
-  rodv_status finish_lane(HostLane& lane, double* out, rodv_stats* st);
+                               const std::vector<uint32_t>& bounds, uint8_t* prec);
+  rodv_status finish_lane(HostLane& lane, double* out, rodv_stats* st, uint8_t* prec);
   int persistent_blocks(const KernelInfo& k) const;
   size_t multi_scratch_rows() const;
   std::string device_key() const;

@@ -140,6 +140,10 @@ struct BatchView {
   const HapDesc* haps;
   const ReadDesc* reads;
   double* out;
+  // Raw mode (null otherwise): out[] receives the scaled likelihood itself
+  // and raw_prec[] the precision that produced it -- 0: FP32, scaled by
+  // 2^120/haplen; 1: FP64, scaled by 2^1020/haplen.
+  uint8_t* raw_prec;
   PriorTables tab;
 };
 

@@ -435,6 +435,7 @@ extern "C" rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32
   v.haps = reinterpret_cast<const HapDesc*>(s + kOffHaps);
   v.reads = reinterpret_cast<const ReadDesc*>(s + kOffReads);
   v.out = out_log10;
+  v.raw_prec = nullptr;
   v.tab.ph2pr_f = reinterpret_cast<const float*>(s + kOffPh2prF);
   v.tab.mm_f = reinterpret_cast<const float*>(s + kOffMmF);
   v.tab.ph2pr_d = reinterpret_cast<const double*>(s + kOffPh2prD);

@@ -955,7 +955,12 @@ struct Forward {
     }
     if (P::kSlots == 2) {
       if (raw >= accept_min) {
-        b.out[ref.out] = log10(raw) - kLog10InitF;
+        if (b.raw_prec) {
+          b.out[ref.out] = raw;
+          b.raw_prec[ref.out] = 0;
+        } else {
+          b.out[ref.out] = log10(raw) - kLog10InitF;
+        }
       } else {
         const uint32_t k = atomicAdd(c.rescue_count, 1u);
         c.rescue_list[k] = ref;
@@ -964,8 +969,13 @@ struct Forward {
       // The reference computes with flush-to-zero on (common.h:58-62), which on
       // x86 also flushes FP64 denormals: a likelihood below the normal FP64
       // range of the 2^1020 scaling becomes 0 and its log10 is -inf.  The GPU's
-      // FP64 keeps denormals, so such a result is mapped to -inf here.
-      b.out[ref.out] = (raw >= kDblMin) ? log10(raw) - kLog10InitD : -CUDART_INF;
+      // FP64 keeps denormals, so such a result is mapped to 0 (-inf) here.
+      if (b.raw_prec) {
+        b.out[ref.out] = raw >= kDblMin ? raw : 0.0;
+        b.raw_prec[ref.out] = 1;
+      } else {
+        b.out[ref.out] = (raw >= kDblMin) ? log10(raw) - kLog10InitD : -CUDART_INF;
+      }
     }
   }
 };

@@ -552,3 +552,38 @@ def test_forced_fp64_device_batch_graph_replays():
     assert np.abs(r1 - oracle.batch_log10(b, oracle.FP64)).max() < 1e-9
     db.free()
     e.close()
+
+
+def test_raw_output_matches_log10_output(engine):
+    """rodv_pairhmm_batch_raw (the inter API's islog10 = false) returns the
+    scaled likelihood and its precision; log10 of it with that precision's
+    offset is the log10 result, FP32 raws agree with the oracle's FP32 sum,
+    and a likelihood below the FP64 normal range comes back as 0 (-inf).
+    The uneven sample is large enough for the pipelined host path (region
+    ranges over three lanes)."""
+    for b in (workloads.make_workload("tiny", scale=4.0),
+              workloads.make_workload("underflow", scale=0.002),
+              workloads.make_workload("uneven", scale=0.05)):
+        want = engine.batch(b)
+        raw, prec = engine.batch_raw(b)
+        assert set(np.unique(prec)) <= {0, 1}
+        off = np.where(prec == 0, float(np.float32(36.1236000061)), 307.050595577260822)
+        with np.errstate(divide="ignore"):
+            got = np.log10(raw) - off
+        fin = np.isfinite(want)
+        assert np.array_equal(fin, np.isfinite(got))
+        assert np.abs(got[fin] - want[fin]).max() < 1e-12
+        assert np.all(raw[prec == 0] >= 1e-28)
+        if b.num_pairs < 5000:
+            f32 = oracle.batch_log10(b, oracle.FP32_RAW)
+            sel = prec == 0
+            assert np.abs(raw[sel] / f32[sel] - 1).max() < 1e-4
+    # forced FP64: every precision byte is 1
+    b = workloads.make_workload("tiny", scale=2.0)
+    raw, prec = engine.batch_raw(b, use_double=True)
+    assert np.all(prec == 1)
+    with np.errstate(divide="ignore"):
+        got = np.log10(raw) - 307.050595577260822
+    want = engine.batch(b, use_double=True)
+    fin = np.isfinite(want)
+    assert np.abs(got[fin] - want[fin]).max() < 1e-12
