@@ -419,7 +419,9 @@ def run_profile(args, local):
                                     scale=args.scale)
     eng = Engine(local)
     if args.tune:
-        eng.autotune()
+        # with --tune-cache, a first run tunes and writes the cache and later
+        # runs (the one ncu profiles) only read it: no tuning launches
+        eng.autotune(cache_path=args.tune_cache or None)
     db = eng.upload(batch)
     for _ in range(args.warmup):
         db.run()
@@ -712,6 +714,9 @@ def main():
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the per-configuration throughput lines (C1, C3-C5)")
     ap.add_argument("--tune", action="store_true", help="profile mode: autotune first")
+    ap.add_argument("--tune-cache", default="",
+                    help="profile mode: tuning cache file (read if it has this device, else "
+                         "written after tuning)")
     ap.add_argument("--ref-seconds", type=float, default=6.0,
                     help="reference arm: wall seconds of CPU work per step")
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
