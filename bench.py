@@ -29,7 +29,9 @@ Reported (see the JSON keys):
 Multi-GPU (torchrun): one process per GPU; every rank computes its own
 workload of the same shape (seed + rank), no collective on the data path;
 the barrier and max-over-ranks timing use torch.distributed.  ``scaling`` is
-weak.  ``--impl reference`` times the reference's CPU path on rank 0 only.
+weak.  ``strong_scaling`` shards one batch of the workload over the ranks by
+region (rodv_shard_plan) and times it the same way.  ``--impl reference``
+times the reference's CPU path on rank 0 only.
 """
 from __future__ import annotations
 
@@ -322,6 +324,29 @@ def run_engine(args, world, rank, local):
     e2e_value = world * cells * len(e2e_ms) / e2e_total / 1e9
     same = float(np.abs(out - results).max())
 
+    # ---- strong scaling (N > 1): one batch, its regions sharded over the ranks ----
+    strong = None
+    if world > 1 and not args.no_strong:
+        from rodv_b200.sharding import shard_plan
+        whole = (batch if rank == 0 else
+                 workloads.make_workload(args.workload, seed=workloads.SEEDS[args.workload],
+                                         scale=args.scale))
+        assign, shard_cells = shard_plan(whole, world)
+        sub = whole.subset(np.nonzero(assign == rank)[0].tolist())
+        sdb = eng.upload(sub)
+        for _ in range(args.warmup):
+            sdb.run()
+        barrier()
+        s_ms = [sdb.run()["device_ms"] for _ in range(args.steps)]
+        barrier()
+        sdb.free()
+        s_total = max_over_ranks(sum(s_ms) / 1e3)
+        strong = {"value": whole.cells() * args.steps / s_total / 1e9, "unit": "GCUPS",
+                  "what": "one batch of the workload, its regions sharded over the ranks by "
+                          "rodv_shard_plan (cells, longest first); device time, max over ranks",
+                  "ms_per_step": s_total / args.steps * 1e3,
+                  "max_shard_cells_frac": float(shard_cells.max() / shard_cells.sum())}
+
     line = None
     if rank == 0:
         fp32_avg_s = sum(fp32_ms) / len(fp32_ms) / 1e3
@@ -380,6 +405,8 @@ def run_engine(args, world, rank, local):
             "clocks": clocks,
             "wall_s_timed": wall,
         }
+        if strong:
+            line["strong_scaling"] = strong
         if plain:
             line["plain_form"] = plain
             line["config"]["C1_plain_speedup"] = plain["speedup"]
@@ -709,6 +736,8 @@ def main():
                     help="CSV of the nvidia-smi clock samples (default: a temporary file)")
     ap.add_argument("--plain-pairs", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-strong", action="store_true",
+                    help="N > 1: skip the strong-scaling measurement")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the per-configuration accuracy samples")
     ap.add_argument("--no-configs", action="store_true",
