@@ -367,6 +367,12 @@ const char* rodv_service_last_error(rodv_service* service);
  * many device and pinned-host allocations of the library are live, so a test
  * can check that a failed call released what it had allocated. */
 rodv_status rodv_fault_inject_alloc(int32_t kind, int64_t nth);
+/* While enabled, long reads' multi-pass sweeps (whose warps wait for one
+ * another's progress, each wait bounded) run with progress publication off
+ * and a short wait limit: every wait runs out, the kernel records it and
+ * returns, and the call fails with RODV_ERR_DEVICE_CHECK.  Tests the expiry
+ * path with no hang and no fault; the device stays usable. */
+rodv_status rodv_fault_inject_wait(int32_t enable);
 void rodv_debug_live_allocations(uint64_t* device, uint64_t* pinned_host);
 
 /* Human-readable name of a status code (static storage). */

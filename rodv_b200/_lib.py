@@ -151,6 +151,7 @@ SIGNATURES = [
     ("rodv_service_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
     ("rodv_fault_inject_alloc", ctypes.c_int32, [ctypes.c_int32, ctypes.c_int64]),
     ("rodv_debug_live_allocations", None, [_u64p, _u64p]),
+    ("rodv_fault_inject_wait", ctypes.c_int32, [ctypes.c_int32]),
     ("rodv_status_string", ctypes.c_char_p, [ctypes.c_int32]),
     ("rodv_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
 ]

@@ -225,6 +225,11 @@ rodv_status rodv_fault_inject_alloc(int32_t kind, int64_t nth) {
   return RODV_OK;
 }
 
+rodv_status rodv_fault_inject_wait(int32_t enable) {
+  rodv::set_wait_fault(enable != 0);
+  return RODV_OK;
+}
+
 void rodv_debug_live_allocations(uint64_t* device, uint64_t* pinned_host) {
   rodv::live_allocations(device, pinned_host);
 }

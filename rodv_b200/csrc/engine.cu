@@ -143,6 +143,20 @@ bool injected_failure(int kind) {
 }  // namespace
 
 void set_alloc_fault(int kind, int64_t nth) { g_fail_countdown[kind].store(nth > 0 ? nth : 0); }
+
+// Testing hook (rodv_fault_inject_wait): multi-pass launches made while it is
+// set publish no progress and give up a wait after kTestWaitPolls polls.
+namespace {
+std::atomic<bool> g_wait_fault{false};
+constexpr uint32_t kTestWaitPolls = 1u << 12;
+void apply_wait_fault(ClassLaunch& cl, int cls) {
+  if (class_multi(cls) && g_wait_fault.load()) {
+    cl.flags |= kLaunchNoPublish;
+    cl.wait_polls = kTestWaitPolls;
+  }
+}
+}  // namespace
+void set_wait_fault(bool on) { g_wait_fault.store(on); }
 void live_allocations(uint64_t* device, uint64_t* pinned) {
   if (device) *device = (uint64_t)g_live[0].load();
   if (pinned) *pinned = (uint64_t)g_live[1].load();
@@ -849,6 +863,7 @@ rodv_status Engine::launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, in
   cl.scratch = class_scratch(plan, a, c);
   cl.scratch_cols = plan.scratch_cols;
   cl.error_flags = a.counts + kCtrError;
+  apply_wait_fault(cl, c);
   const int per_block = k.items_per_block;
   const int need = (int)((n + per_block - 1) / per_block);
   int blocks = std::max(1, std::min(persistent_blocks(k), need));
@@ -873,6 +888,7 @@ rodv_status Engine::launch_fp64_class(const PackedPlan& plan, uint8_t* dbase, in
   cl.scratch = class_scratch(plan, a, c);
   cl.scratch_cols = plan.scratch_cols;
   cl.error_flags = a.counts + kCtrError;
+  apply_wait_fault(cl, c);
   const int need = (int)((plan.pairs[c] + k.items_per_block - 1) / k.items_per_block);
   const int blocks = std::max(1, std::min(persistent_blocks(k), need));
   void* args[] = {&a.view, &cl};

@@ -46,6 +46,7 @@ enum CounterBlock : int {
 // Testing hooks behind rodv_fault_inject_alloc / rodv_debug_live_allocations:
 // kind 0 = device (cudaMalloc), 1 = pinned host (cudaMallocHost).
 void set_alloc_fault(int kind, int64_t nth);
+void set_wait_fault(bool on);
 void live_allocations(uint64_t* device, uint64_t* pinned);
 
 struct DeviceMem {

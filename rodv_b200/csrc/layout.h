@@ -158,7 +158,14 @@ struct ClassLaunch {
   float* scratch;              // MULTI: per resident warp boundary-row buffer
   uint32_t scratch_cols;       // columns per warp buffer (max hap len + 40)
   uint32_t* error_flags;       // bit set by a kernel that hit a bad descriptor
+  uint32_t flags;              // kLaunch* bits
+  uint32_t wait_polls;         // pipelined sweeps: polls before a wait gives up (0: default)
 };
+
+// ClassLaunch::flags.  Testing hook: the producers of a pipelined sweep
+// publish no progress, so every consumer's wait runs out (its expiry path is
+// tested without a fault).
+constexpr uint32_t kLaunchNoPublish = 1u;
 
 enum ErrorFlag : uint32_t {
   kErrBadLength = 1u,   // a pair with zero or over-limit length reached a kernel

@@ -89,11 +89,12 @@ struct PipeForward {
 
   // The whole warp waits until boundary row `row` is published up to `want`;
   // false (in every lane) when the item stopped meanwhile or the wait expired.
-  __device__ static bool wait_prog(Ctl& ctl, int row, uint32_t want, uint32_t* err) {
+  __device__ static bool wait_prog(Ctl& ctl, int row, uint32_t want, uint32_t* err,
+                                   uint32_t polls) {
     for (uint32_t k = 0;; ++k) {
       if (__all_sync(kFullMask, ld_acquire_cta(&ctl.prog[row]) >= want)) return true;
       if (stopped(ctl)) return false;
-      if (k >= kWaitPolls) {
+      if (k >= polls) {
         if ((threadIdx.x & (kWarp - 1)) == 0) {
           atomicOr(err, kErrWaitTimeout);
           atomicExch(&ctl.stop, kStopFailed);
@@ -154,6 +155,8 @@ struct PipeForward {
     const uint32_t L[2] = {sl[0].L, sl[1].L};
     const uint64_t row_off[2] = {sl[0].row_off, sl[1].row_off};
     Cell* ring = reinterpret_cast<Cell*>(table + F::Shape::kBytesPerWarp / 16);
+    const uint32_t polls = c.wait_polls ? c.wait_polls : kWaitPolls;
+    const bool publish = (c.flags & kLaunchNoPublish) == 0;
 
     for (uint32_t p = (uint32_t)warp; p < passes; p += W) {
       if (stopped(ctl)) break;
@@ -168,7 +171,7 @@ struct PipeForward {
         const uint32_t first = (uint32_t)k * kWarp + 1u;
         if (first <= H) {
           const uint32_t upto = first + kWarp - 1 < H ? first + kWarp - 1 : H;
-          if (!wait_prog(ctl, in_row, enc(p - 1, upto), c.error_flags)) return false;
+          if (!wait_prog(ctl, in_row, enc(p - 1, upto), c.error_flags, polls)) return false;
         }
         const uint32_t idx = first + (uint32_t)lane;
         if (idx < c.scratch_cols) {
@@ -237,7 +240,7 @@ struct PipeForward {
             Cell cell;
             cell.m = M[R - 1]; cell.i = I[R - 1]; cell.d = D[R - 1];
             dst[col] = cell;
-            if ((col & (kWarp - 1)) == 0 || col == (int)H) {
+            if (publish && ((col & (kWarp - 1)) == 0 || col == (int)H)) {
               __threadfence_block();
               st_release_cta(&ctl.prog[out_row], enc(p, (uint32_t)col));
             }

@@ -111,3 +111,25 @@ def test_service_create_out_of_memory(kind):
     sv = Service(0)  # creation works again
     sv.close()
     assert _live() == base
+
+
+@pytest.mark.parametrize("use_double", [False, True])
+def test_pipelined_wait_expiry_is_reported_and_device_stays_usable(engine, use_double):
+    """Long reads' multi-pass sweeps run one item's passes on several warps
+    that wait for one another's published progress, each wait bounded.  With
+    the testing hook on, nothing is published: every wait runs out, the kernel
+    records kErrWaitTimeout and returns, the call fails with
+    RODV_ERR_DEVICE_CHECK, and the same engine then computes the batch
+    correctly (no hang, no fault, the context stays usable)."""
+    b = workloads.make_workload("long", scale=0.002)   # 4 long pairs, several passes each
+    want = engine.batch(b, use_double=use_double)
+    lib = _lib.load()
+    assert lib.rodv_fault_inject_wait(1) == 0
+    try:
+        with pytest.raises(RodvError) as ei:
+            engine.batch(b, use_double=use_double)
+    finally:
+        lib.rodv_fault_inject_wait(0)
+    assert ei.value.status == 8, ei.value       # RODV_ERR_DEVICE_CHECK
+    assert "error flags 16" in str(ei.value)     # kErrWaitTimeout
+    assert np.array_equal(engine.batch(b, use_double=use_double), want)
