@@ -20,9 +20,12 @@ namespace rodv {
 constexpr int kSinglePassClasses = kMaxRowsPerLane * 2;
 constexpr int kNumClasses = kSinglePassClasses + 2;
 
+// A single-pass class holds reads of up to 32R - 1 bases (R = floor(L/32) + 1):
+// the sweep's last row is always a pass-through row, so one running sum
+// gives the result.  Reads of 256 bases and more are multi-pass.
 inline int class_of(uint32_t read_len, bool uniform) {
-  if (read_len <= (uint32_t)kPassRows) {
-    const int R = (int)((read_len + kWarp - 1) / kWarp);
+  if (read_len < (uint32_t)kPassRows) {
+    const int R = (int)(read_len / kWarp) + 1;
     return (R - 1) * 2 + (uniform ? 1 : 0);
   }
   return kSinglePassClasses + (uniform ? 1 : 0);

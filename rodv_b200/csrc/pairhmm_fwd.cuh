@@ -228,10 +228,11 @@ struct SlotInfo {
 
 // Per-group shared memory of a chain sweep beyond the emission table: the
 // column of the separator after each haplotype (the last one is the virtual
-// separator just past the chain's end), and the last lane's two running sums
-// (M, I of the last read row; x and y halves) at the end of each haplotype.
+// separator just past the chain's end), and the last lane's running sum (I of
+// its last row, a pass-through row; x and y halves) at the end of each
+// haplotype.
 struct ChainMeta {
-  float4 acc[kChainHaps];
+  float2 acc[kChainHaps];  // column sums of the last lane's last row (I, x and y halves)
   uint32_t sep[kChainHaps + 4];  // kChainHaps + 1 used; padded to 16 bytes
 };
 
@@ -822,7 +823,7 @@ struct Forward {
                                                           co_next != co + hl + 1));
     const uint32_t Lmax = rx.len > ry.len ? rx.len : ry.len;
     const bool bad = bad_hap || hl > it.norm_len || n == 0 || n > (uint32_t)kGroupHaps ||
-                     rx.len == 0 || ry.len == 0 || Lmax > (uint32_t)(GROUP * R);
+                     rx.len == 0 || ry.len == 0 || Lmax >= (uint32_t)(GROUP * R);
     if (__any_sync(kFullMask, bad)) {
       if (lane == 0) atomicOr(c.error_flags, kErrChain);
       return;
@@ -861,7 +862,11 @@ struct Forward {
     const uint8_t* hx = b.hap_codes + co0 - gl;
     uint32_t hi = 0;                          // this lane's haplotype in the chain
     int nxt = (int)meta->sep[0] + gl;         // step at which this lane is at the next separator
-    V acc_m = P::zero(), acc_i = P::zero();
+    // Reads of a single-pass class are shorter than the rows the sweep holds
+    // (class_of), so the last lane's last row is a pass-through row: its M is
+    // 0 and its I carries the read's last-row value; one running sum
+    // (of I) gives the result.
+    V acc_i = P::zero();
     // through the virtual end separator of the longer chain, for the last lane
     const int nsteps = (int)span + GROUP;
     // A lane of the shorter chain of a two-group warp keeps stepping past its
@@ -899,14 +904,13 @@ struct Forward {
         load_emission(table, lane, code, 0u, e);
         cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr, t_last);
       }
-      acc_m = P::fma(t_last, e[R - 1], acc_m);  // += M[R-1], one rounding
+      (void)t_last;
       acc_i = P::add(acc_i, I[R - 1]);
       if (s == nxt) {  // this lane just computed a separator column
 #pragma unroll
         for (int k = 0; k < R; ++k) D[k] = P::zero();
         if (gl == GROUP - 1) {
-          meta->acc[hi] = make_float4(P::sx(acc_m), P::sy(acc_m), P::sx(acc_i), P::sy(acc_i));
-          acc_m = P::zero();
+          meta->acc[hi] = make_float2(P::sx(acc_i), P::sy(acc_i));
           acc_i = P::zero();
         }
         ++hi;
@@ -915,21 +919,18 @@ struct Forward {
     }
     __syncwarp();
     if (active && (uint32_t)gl < n) {
-      const float4 a = meta->acc[gl];
+      const float2 a = meta->acc[gl];
       const double ratio = (double)(P::init_const() / (S)hl) / (double)init_s;
       const uint32_t hap = it.hap_start + gl;
       const uint32_t out = it.out_x + (uint32_t)gl * it.stride;
       double res_x, res_y = 0.0;
       double amin_x = (double)kMinAcceptedF, amin_y = (double)kMinAcceptedF;
-      if (kScaled) {
-        res_x = scaled_result(b, it.read_x, rx.len, GROUP * R, a.x, a.z, &amin_x);
-        if (has_y) res_y = scaled_result(b, it.read_y, ry.len, GROUP * R, a.y, a.w, &amin_y);
-      } else if (UNIFORM) {
-        res_x = uniform_gapm(b, it.read_x) * a.x + a.z;
-        if (has_y) res_y = uniform_gapm(b, it.read_y) * a.y + a.w;
-      } else {
-        res_x = a.x + a.z;
-        res_y = a.y + a.w;
+      if (kScaled) {  // the pass-through row holds (M_L + I_L)/gapm: the sum / mi
+        res_x = scaled_result(b, it.read_x, rx.len, GROUP * R, 0.f, a.x, &amin_x);
+        if (has_y) res_y = scaled_result(b, it.read_y, ry.len, GROUP * R, 0.f, a.y, &amin_y);
+      } else {        // the pass-through row holds M_L + I_L (its M is 0)
+        res_x = a.x;
+        res_y = a.y;
       }
       finish(b, c, PairRef{hap, it.read_x, out}, res_x * ratio, amin_x);
       if (has_y)
