@@ -61,11 +61,14 @@
 #include <math_constants.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "layout.h"
 
 namespace rodv {
 
 constexpr unsigned kFullMask = 0xffffffffu;
+constexpr int kStepBlock = 8;  // chain sweeps: steps per block (unrolled)
 constexpr float kMinAcceptedF = 1e-28f;
 // log10 offsets of the two scaling constants, spelled as the reference
 // spells them (pairhmm/inter/pairhmm_inter_api.h:8-15): the FP32 one is a float
@@ -128,7 +131,8 @@ struct F32x2 {
   __device__ __forceinline__ static V zero() { return make_float2(0.f, 0.f); }
   __device__ __forceinline__ static V make(S x, S y) { return make_float2(x, y); }
   __device__ __forceinline__ static V shfl_up(V v) {
-    return make_float2(__shfl_up_sync(kFullMask, v.x, 1), __shfl_up_sync(kFullMask, v.y, 1));
+    // one 64-bit shuffle of the register pair (no moves to assemble the pair)
+    return f2_value(__shfl_up_sync(kFullMask, f2_bits(v), 1));
   }
   __device__ __forceinline__ static S sx(V v) { return v.x; }
   __device__ __forceinline__ static S sy(V v) { return v.y; }
@@ -272,8 +276,7 @@ struct Forward {
   // of the same group).
   __device__ __forceinline__ static V group_shfl_up(V v) {
     if constexpr (P::kSlots == 2) {
-      return P::make(__shfl_up_sync(kFullMask, P::sx(v), 1, GROUP),
-                     __shfl_up_sync(kFullMask, P::sy(v), 1, GROUP));
+      return f2_value(__shfl_up_sync(kFullMask, f2_bits(v), 1, GROUP));
     } else {
       return P::shfl_up(v);
     }
@@ -875,11 +878,13 @@ struct Forward {
     const int last_s = (int)ncols + gl;
 
     // the haplotype code of the next step is loaded one step ahead (the
-    // emission loads wait on it); at most one byte past the last step's,
-    // inside the code array's tail padding
+    // emission loads wait on it); the sweep runs in blocks of kStepBlock
+    // steps, up to kStepBlock - 1 steps past the last one, whose columns
+    // (past every lane's last separator) change no stored sum, and whose code
+    // reads stay inside the code array's tail padding
     uint32_t code_next = hx[0];
-#pragma unroll 2
-    for (int s = 0; s < nsteps; ++s) {
+    // one step; CHECK: whether a lane may reach a separator column in it
+    auto step = [&](int s, auto check) {
       V e[R], t_last;
       const uint32_t code = code_next;
       code_next = hx[kGroups > 1 ? min(s + 1, last_s) : s + 1];
@@ -906,15 +911,31 @@ struct Forward {
       }
       (void)t_last;
       acc_i = P::add(acc_i, I[R - 1]);
-      if (s == nxt) {  // this lane just computed a separator column
+      if constexpr (decltype(check)::value) {
+        if (s == nxt) {  // this lane just computed a separator column
 #pragma unroll
-        for (int k = 0; k < R; ++k) D[k] = P::zero();
-        if (gl == GROUP - 1) {
-          meta->acc[hi] = make_float2(P::sx(acc_i), P::sy(acc_i));
-          acc_i = P::zero();
+          for (int k = 0; k < R; ++k) D[k] = P::zero();
+          if (gl == GROUP - 1) {
+            meta->acc[hi] = make_float2(P::sx(acc_i), P::sy(acc_i));
+            acc_i = P::zero();
+          }
+          ++hi;
+          nxt = (int)meta->sep[hi] + gl;
         }
-        ++hi;
-        nxt = (int)meta->sep[hi] + gl;
+      }
+    };
+    // A lane meets a separator once per haplotype, so most blocks of steps
+    // hold none for any lane of the warp: those run without the per-step
+    // separator test (a warp-uniform choice per block).
+    const int nblocks = (nsteps + kStepBlock - 1) / kStepBlock;
+#pragma unroll 1
+    for (int s0 = 0; s0 < nblocks * kStepBlock; s0 += kStepBlock) {
+      if (__any_sync(kFullMask, nxt < s0 + kStepBlock)) {
+#pragma unroll
+        for (int i = 0; i < kStepBlock; ++i) step(s0 + i, std::true_type{});
+      } else {
+#pragma unroll
+        for (int i = 0; i < kStepBlock; ++i) step(s0 + i, std::false_type{});
       }
     }
     __syncwarp();

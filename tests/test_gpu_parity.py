@@ -574,9 +574,9 @@ def test_raw_output_matches_log10_output(engine):
         assert np.array_equal(fin, np.isfinite(got))
         assert np.abs(got[fin] - want[fin]).max() < 1e-12
         assert np.all(raw[prec == 0] >= 1e-28)
-        if b.num_pairs < 5000:
+        sel = prec == 0
+        if b.num_pairs < 5000 and sel.any():
             f32 = oracle.batch_log10(b, oracle.FP32_RAW)
-            sel = prec == 0
             assert np.abs(raw[sel] / f32[sel] - 1).max() < 1e-4
     # forced FP64: every precision byte is 1
     b = workloads.make_workload("tiny", scale=2.0)
