@@ -1489,8 +1489,9 @@ struct TuneBatch {
   }
 };
 
+// one_in: one base in `one_in` of a read differs from its haplotype.
 void make_tune_batch(TuneBatch& tb, std::mt19937& rng, int regions, int haps, int reads,
-                     uint32_t H, uint32_t L, bool uni) {
+                     uint32_t H, uint32_t L, bool uni, uint32_t one_in = 100) {
   const char* acgt = "ACGT";
   for (int g = 0; g < regions; ++g) {
     rodv_region r{(uint32_t)tb.ho.size(), (uint32_t)haps, (uint32_t)tb.ro.size(),
@@ -1507,7 +1508,7 @@ void make_tune_batch(TuneBatch& tb, std::mt19937& rng, int regions, int haps, in
       tb.rl.push_back(L);
       const uint32_t st = rng() % (H - std::min(L, H) + 1);
       for (uint32_t j = 0; j < L; ++j) {
-        tb.rb.push_back(j + st < H && rng() % 100 ? base[j + st] : acgt[rng() % 4]);
+        tb.rb.push_back(j + st < H && rng() % one_in ? base[j + st] : acgt[rng() % 4]);
         tb.q.push_back(10 + rng() % 31);
         tb.ins.push_back(uni ? 45 : 20 + rng() % 26);
         tb.del.push_back(uni ? 45 : 20 + rng() % 26);
@@ -1553,8 +1554,12 @@ rodv_status Engine::autotune(const char* cache_path, int force, int32_t* variant
     const bool multi = class_multi(c), uni = class_uniform(c);
     TuneBatch tb;
     if (multi) {
-      // long pairs: several waves of the largest grid of one item per block
-      make_tune_batch(tb, rng, num_sms_ * 4, 1, 2, 3000, 1500, uni);
+      // long pairs, several waves of the largest grid of one item per block:
+      // half the regions with reads of 1% differences (the FP32 sweep runs
+      // every pass), half with 8% (it stops after the first passes and the
+      // pairs go to FP64), so the choice weighs both kinds of long read
+      make_tune_batch(tb, rng, num_sms_ * 2, 1, 2, 3000, 1500, uni, 100);
+      make_tune_batch(tb, rng, num_sms_ * 2, 1, 2, 3000, 1500, uni, 12);
     } else {
       // Enough items that every warp of the largest grid takes several (chain
       // items of 4 haplotypes: ~8), so the timing reflects per-item throughput

@@ -696,7 +696,7 @@ struct Forward {
       // array's tail padding
       uint32_t cx_next = hx[0], cy_next = kSameHap ? 0u : (uint32_t)hy[0];
 
-#pragma unroll 2
+#pragma unroll 4
       for (int s = 0; s < nsteps; ++s) {
         const uint32_t cx = cx_next, cy = cy_next;
         cx_next = hx[s + 1];

@@ -201,7 +201,8 @@ struct PipeForward {
       V acc_m = P::zero(), acc_i = P::zero();
       S frozen_m = 0, frozen_i = 0;
 
-#pragma unroll 2
+      // four steps per loop iteration (C3's FP64 pass: 10.2 ms at two, 9.3 at four)
+#pragma unroll 4
       for (int s = 0; s < nsteps; ++s) {
         if (!alive) break;
         const uint32_t cx = cx_next, cy = cy_next;
