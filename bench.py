@@ -104,6 +104,42 @@ def step_traffic_bytes(workload, scale):
     return int(f["fp32_step_traffic_bytes"]), f.get("traffic_note", "")
 
 
+def chain_class_cells(batch):
+    """Cells each single-pass chain class computes in the FP32 pass, keyed by
+    (rows per lane, uniform gaps): the packer's pairing restated (engine.cu,
+    pack): a region's single-pass reads sorted by (uniform gaps, length) pair
+    up neighbour by neighbour, and a pair's chain items are of the class of
+    its longer read (uniform only if both are); an odd last read goes to the
+    two-haplotype kernel instead.  Scales a one-class traffic capture to a
+    step."""
+    rl = batch.read_lengths.astype(np.int64)
+    hl = batch.hap_lengths.astype(np.int64)
+    ro = batch.read_offsets.astype(np.int64)
+    const = np.ones(len(rl), dtype=bool)
+    first = {}
+    for name in ("ins_quals", "del_quals", "gcp_quals"):
+        q = getattr(batch, name).astype(np.int64) & 127
+        first[name] = q[ro]
+        if len(q):
+            const &= (np.maximum.reduceat(q, ro) == np.minimum.reduceat(q, ro))
+    ins, gcp = first["ins_quals"], first["gcp_quals"]
+    uni = (const & (ins == first["del_quals"]) & (gcp != 0) &
+           (10.0 ** (-ins / 10.0) * (1.0 - 10.0 ** (-gcp / 10.0)) >= 1e-6))
+    key = (uni.astype(np.int64) << 20) | rl
+    out = {}
+    for rg in batch.regions:
+        h0, r0 = int(rg["hap_start"]), int(rg["read_start"])
+        hsum = int(hl[h0:h0 + int(rg["num_haps"])].sum())
+        reads = np.arange(r0, r0 + int(rg["num_reads"]))
+        single = reads[rl[reads] < 256]
+        s = single[np.argsort(key[single], kind="stable")]
+        for k in range(0, len(s) - 1, 2):
+            x, y = s[k], s[k + 1]
+            c = (int(max(rl[x], rl[y])) // 32 + 1, bool(uni[x] and uni[y]))
+            out[c] = out.get(c, 0) + hsum * int(rl[x] + rl[y])
+    return out
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 

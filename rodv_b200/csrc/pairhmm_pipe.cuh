@@ -8,40 +8,61 @@
 // longest pairs of a batch set the length of the whole launch.  Here the W
 // warps of a block take one work item together: warp w sweeps passes w, w+W,
 // w+2W, ...  Lane 31 of the warp on pass p writes the pass's last row into a
-// boundary row in global memory and publishes, every 32 columns, how far it
-// has come; lane 0 of the warp on pass p+1 reads that row through the
-// shared-memory ring of the single-warp sweep (cp.async, 32 columns ahead),
-// waiting for the publication before each chunk.  Pass p+1 thus trails pass p
-// by about 100 steps instead of a whole pass, and the item's sweep takes
-// about ceil(P/W) passes plus (W-1) x 100 steps.
+// boundary row in global memory and publishes, after every 32 steps, how far
+// it has come; lane 0 of the warp on pass p+1 reads that row through a
+// shared-memory ring (cp.async, 32 columns ahead), waiting for the
+// publication before each chunk.  Pass p+1 thus trails pass p by about 100
+// steps instead of a whole pass, and the item's sweep takes about ceil(P/W)
+// passes plus (W-1) x 100 steps.
+//
+// What crosses a pass boundary is what the lanes of a warp hand each other.
+// In the scaled form (uniform gaps) that is two values per column: the M term
+// of the row below, t = (mm/c) M~ + I^ + D^ (used one column later), and the
+// row below's I^ = ii' I^ + M~ (ii' of the row below), both computed by the
+// lane above with the operations the lane below would apply, so the results
+// are bitwise those of a three-value hand-over of (M~, I^, D^).  Other forms
+// hand over (M, I, D).  A boundary cell is 16 or 24 bytes.
 //
 // Boundary rows.  A block owns W+1 rows; pass p writes row p mod (W+1) and
 // reads row (p-1) mod (W+1).  The next pass to write a row, p+W+1, runs on
 // the same warp as p+1, the row's only reader, after p+1 has finished, so a
 // producer never waits for a consumer.  Every wait is a consumer (pass p)
-// waiting for its producer (pass p-1): waits point to strictly earlier passes,
-// so they cannot form a cycle.  Each wait also gives up after a bounded number
-// of polls, sets kErrWaitTimeout and stops the item, so a kernel always ends.
+// waiting for its producer (pass p-1): waits point to strictly earlier
+// passes, so they cannot form a cycle.  Each wait also gives up after a
+// bounded number of polls, sets kErrWaitTimeout and stops the item, so a
+// kernel always ends.  A row starts with kPad cells
+// before its column 0: lane 31 stores its hand-over every step, the first 31
+// of which are columns <= 0 (zeros, never read), so no store needs a column
+// test.
 //
 // Progress words live in shared memory: (pass << 17) | column, written with a
 // CTA-scope release by the producing lane after its row stores (and a block
 // fence), read with a CTA-scope acquire by every lane of the consumer before
-// it copies the chunk.  Both warps are in one block, so they share the SM's
+// it copies the chunk.  The warps are in one block, so they share the SM's
 // L1 and the CTA scope suffices.
 //
 // FP32 items stop early as in the single-warp sweep: after each pass but the
-// last, the warp that swept it bounds the likelihood by the sum of the row it
-// wrote (Forward::row_bound_rejects); once both slots are below the acceptance
-// bound the item stops on every warp and both pairs go to FP64.  The bound is
-// exact, so the rescued pairs and every result are those of the full sweep.
+// last, the warp that swept it bounds the likelihood by the sum over the row
+// it wrote (rejects(), the bound of Forward::row_bound_rejects restated for
+// the hand-over cells); once both slots are below the acceptance bound the
+// item stops on every warp and both pairs go to FP64.  The bound is exact, so
+// the rescued pairs and every result are those of the full sweep.  (Holding
+// pass 1 back until pass 0's verdict, so that a rejected item costs one pass
+// instead of the passes in flight, made no difference on 2,000 long pairs
+// that all go to FP64, C3: 2.92 ms FP32 pass either way, since the warps of
+// these latency-bound sweeps leave issue slots free; at a quarter of the
+// pairs it was slower, 1.34 against 1.19 ms.)
 //
 // Results are committed after a block barrier at the end of the item: by the
 // warp that swept the last pass, or, for a rejected item, as FP64 rescues.
 // The per-cell arithmetic is the single-warp sweep's (Forward::cells), and the
 // pass count (pipe_passes, layout.h) leaves at least one pass-through row at
-// the end, so a result is always the column sum of a pass-through row: it
-// depends neither on W nor on the strip height R nor on the item's other read.
+// the end, so a result is always the column sum of the I of a pass-through
+// row (its M is 0): it depends neither on W nor on the strip height R nor on
+// the item's other read.
 #pragma once
+#include <type_traits>
+
 #include "pairhmm_fwd.cuh"
 
 namespace rodv {
@@ -60,14 +81,25 @@ __device__ __forceinline__ void st_release_cta(uint32_t* p, uint32_t v) {
                "r"(v)
                : "memory");
 }
+// cp.async of 16 bytes global -> shared (L2 only); both addresses 16-byte aligned
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned dst = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gmem) : "memory");
+}
 
 template <class P, int R, bool UNIFORM, bool SAME, int MINB, int W>
 struct PipeForward {
   using F = Forward<P, R, UNIFORM, true, SAME, MINB>;
   using V = typename P::V;
   using S = typename P::S;
-  using Cell = typename F::BoundaryCell;
+  static constexpr bool kTwo = F::kScaled;  // two-value hand-over (t, i)
+  struct HandCell {
+    V t, i;
+  };
+  using Cell = typename std::conditional<kTwo, HandCell, typename F::BoundaryCell>::type;
+  static_assert(sizeof(Cell) <= 24, "the engine sizes boundary rows at 24 bytes a cell");
   static constexpr int kRows = W + 1;                   // boundary rows per block
+  static constexpr int kPad = kWarp;                    // cells before column 0 of a row
   static constexpr int kSmemPerWarp = F::kSmemPerWarp;  // emission table + cell ring
   // polls of a progress word (about 100 ns each) before a wait gives up
   static constexpr uint32_t kWaitPolls = 1u << 24;
@@ -87,12 +119,12 @@ struct PipeForward {
     return __any_sync(kFullMask, *reinterpret_cast<volatile uint32_t*>(&ctl.stop) != 0u);
   }
 
-  // The whole warp waits until boundary row `row` is published up to `want`;
-  // false (in every lane) when the item stopped meanwhile or the wait expired.
-  __device__ static bool wait_prog(Ctl& ctl, int row, uint32_t want, uint32_t* err,
+  // The whole warp waits until *word >= want; false (in every lane) when the
+  // item stopped meanwhile or the wait expired (which stops the item).
+  __device__ static bool wait_word(Ctl& ctl, const uint32_t* word, uint32_t want, uint32_t* err,
                                    uint32_t polls) {
     for (uint32_t k = 0;; ++k) {
-      if (__all_sync(kFullMask, ld_acquire_cta(&ctl.prog[row]) >= want)) return true;
+      if (__all_sync(kFullMask, ld_acquire_cta(word) >= want)) return true;
       if (stopped(ctl)) return false;
       if (k >= polls) {
         if ((threadIdx.x & (kWarp - 1)) == 0) {
@@ -106,22 +138,63 @@ struct PipeForward {
     }
   }
 
+  // The FP32 early-rejection decision after a pass (the same value in every
+  // lane), from the hand-over cells of the pass's last row r.  With c = mi
+  // gapm, t = (mm/gapm) M~/mi + I^ + D^ >= min(1, mm/gapm) (M~/mi + I^), so
+  // max(1, gapm/mm) sum_j t bounds the sum Forward::row_bound_rejects bounds
+  // the likelihood by (sum M~/mi + sum I^, rows r < L); a pass-through row
+  // (r >= L) has M~ = D^ = 0 and t = I^, and its bound is sum t / mi.  The
+  // acceptance test and its 1e-6 margin are the same.
+  __device__ static bool rejects(const BatchView& b, const ClassLaunch& c, const Cell* row0,
+                                 const uint32_t (&H)[2], const uint32_t (&L)[2], uint32_t row,
+                                 int lane, uint32_t item) {
+    if constexpr (!kTwo) {
+      return F::row_bound_rejects(b, c, row0, H, L, row, lane, item);
+    } else {
+      V st = P::zero();
+      for (uint32_t col = 1 + (uint32_t)lane; col <= H[0]; col += kWarp) {
+        const V t = row0[col].t;
+        st = P::add(st, P::make(P::sx(t), col <= H[1] ? P::sy(t) : S(0)));
+      }
+      double sum[2] = {(double)P::sx(st), (double)P::sy(st)};
+#pragma unroll
+      for (int d = 16; d >= 1; d /= 2) {
+        sum[0] += __shfl_xor_sync(kFullMask, sum[0], d);
+        sum[1] += __shfl_xor_sync(kFullMask, sum[1], d);
+      }
+      PairRef refs[2];
+      F::load_refs(c, item, refs);
+      bool rejected = true;
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        if (s == 1 && refs[1].read == kNoPair) continue;
+        const uint32_t w = b.read_rows[b.reads[refs[s].read].row_off];
+        const S* ph2pr = Tables<S>::ph2pr(b.tab);
+        const double mi = (double)__ldg(ph2pr + rw_ins(w));
+        const double gapm = 1.0 - (double)__ldg(ph2pr + rw_gcp(w));
+        const double mm = (double)row_priors<S>(w, b.tab).mm;
+        const double bound = row < L[s] ? (gapm > mm ? gapm / mm : 1.0) * sum[s] : sum[s] / mi;
+        const double amin = (double)kMinAcceptedF / (mi * gapm);  // as scaled_result's
+        rejected = rejected && mm > 0.0 && bound >= 0.0 && bound < amin * 1e-6;
+      }
+      return rejected;
+    }
+  }
+
   // What the warp of the item's last pass keeps for the commit.
   struct Sums {
-    V acc_m, acc_i;
-    S frozen_m, frozen_i;
+    V acc;          // column sum of the I of the last row (a pass-through row)
+    S frozen;       // slot y's sum at its own last column (two-haplotype items)
     uint32_t passes;
-    bool ok;  // the item's descriptors were valid
+    bool ok;        // the item's descriptors were valid
   };
 
   // This warp's passes of work item `item`.
   __device__ static Sums run(const BatchView& b, const ClassLaunch& c, uint32_t item, int warp,
                              int lane, uint4* table, Ctl& ctl, Cell* rows) {
     Sums out;
-    out.acc_m = P::zero();
-    out.acc_i = P::zero();
-    out.frozen_m = 0;
-    out.frozen_i = 0;
+    out.acc = P::zero();
+    out.frozen = 0;
     out.passes = 0;
     out.ok = false;
     PairRef refs[2];
@@ -161,25 +234,33 @@ struct PipeForward {
     for (uint32_t p = (uint32_t)warp; p < passes; p += W) {
       if (stopped(ctl)) break;
       const bool last = p + 1 == passes;
+      const bool store = !last && lane == kWarp - 1;
       const int out_row = (int)(p % kRows);
       const int in_row = (int)((p + kRows - 1) % kRows);
-      Cell* dst = rows + (size_t)out_row * c.scratch_cols;
-      const Cell* src = rows + (size_t)in_row * c.scratch_cols;
+      Cell* const out_cells = rows + (size_t)out_row * c.scratch_cols + kPad;  // column 0
+      // lane 31's step s holds column s - 30 after the step
+      Cell* const dst = out_cells - (kWarp - 2);
+      const Cell* const src = rows + (size_t)in_row * c.scratch_cols + kPad;
       // cells of steps [32 k, 32 k + 32) from the previous pass's row
       // (columns 32 k + 1 .. 32 k + 32), copied once they are published
       auto fetch_chunk = [&](int k) -> bool {
         const uint32_t first = (uint32_t)k * kWarp + 1u;
         if (first <= H) {
           const uint32_t upto = first + kWarp - 1 < H ? first + kWarp - 1 : H;
-          if (!wait_prog(ctl, in_row, enc(p - 1, upto), c.error_flags, polls)) return false;
+          if (!wait_word(ctl, &ctl.prog[in_row], enc(p - 1, upto), c.error_flags, polls))
+            return false;
         }
         const uint32_t idx = first + (uint32_t)lane;
-        if (idx < c.scratch_cols) {
+        if (idx + kPad < c.scratch_cols) {
           Cell* d = ring + (k & 1) * kWarp + lane;
           const Cell* s = src + idx;
-          cp_async8(&d->m, &s->m);
-          cp_async8(&d->i, &s->i);
-          cp_async8(&d->d, &s->d);
+          if constexpr (kTwo) {
+            cp_async16(d, s);
+          } else {
+            cp_async8(&d->m, &s->m);
+            cp_async8(&d->i, &s->i);
+            cp_async8(&d->d, &s->d);
+          }
         }
         cp_async_commit();
         return true;
@@ -190,69 +271,99 @@ struct PipeForward {
       V M[R], I[R], D[R];
 #pragma unroll
       for (int k = 0; k < R; ++k) M[k] = I[k] = D[k] = P::zero();
-      V dg_m = P::zero(), dg_i = P::zero(), dg_d = P::zero();
-      if (lane == 0 && p == 0) dg_d = init;
-      const uint8_t* hx = sl[0].hap - lane;
-      const uint8_t* hy = sl[1].hap - lane;
       const bool from_ring = p > 0;
       bool alive = true;
-      if (from_ring) alive = fetch_chunk(0);
-      uint32_t cx_next = hx[0], cy_next = F::kSameHap ? 0u : (uint32_t)hy[0];
-      V acc_m = P::zero(), acc_i = P::zero();
-      S frozen_m = 0, frozen_i = 0;
+      if (from_ring) {
+        alive = fetch_chunk(0);
+      } else {
+        // pass 0: lane 0's row above is row 0 of the DP at every column
+        Cell top;
+        if constexpr (kTwo) {
+          top.t = init; top.i = P::zero();
+        } else {
+          top.m = P::zero(); top.i = P::zero(); top.d = init;
+        }
+        ring[lane] = top;
+        ring[kWarp + lane] = top;
+      }
+      __syncwarp();
+      uint32_t cx_next = sl[0].hap[-lane];
+      uint32_t cy_next = F::kSameHap ? 0u : (uint32_t)sl[1].hap[-lane];
+      const uint8_t* hx = sl[0].hap - lane + 1;  // code of the step after s: hx[s]
+      const uint8_t* hy = sl[1].hap - lane + 1;
+      V acc = P::zero();
+      S frozen = 0;
+      // two-value form: this lane's hand-over for the lane below, and the M
+      // term of its first row carried to the next column
+      V h_t = P::zero(), h_i = P::zero();
+      V dg_t = (lane == 0 && p == 0) ? init : P::zero();
+      // three-value form: the row above at the previous column
+      V dg_m = P::zero(), dg_i = P::zero(), dg_d = (lane == 0 && p == 0) ? init : P::zero();
 
-      // four steps per loop iteration (C3's FP64 pass: 10.2 ms at two, 9.3 at four)
-#pragma unroll 4
-      for (int s = 0; s < nsteps; ++s) {
-        if (!alive) break;
-        const uint32_t cx = cx_next, cy = cy_next;
-        cx_next = hx[s + 1];
-        if (!F::kSameHap) cy_next = hy[s + 1];
-        if ((s & (kWarp - 1)) == 0) {
-          if (from_ring) {
-            cp_async_wait_all();  // this chunk's cells
-            __syncwarp();
-            if (!fetch_chunk(s / kWarp + 1)) {
-              alive = false;
-              break;
-            }
-          } else if (stopped(ctl)) {
+      const int nchunks = (nsteps + kWarp - 1) / kWarp;
+      for (int k = 0; k < nchunks; ++k) {
+        if (from_ring) {
+          cp_async_wait_all();  // this chunk's cells
+          __syncwarp();
+          if (!fetch_chunk(k + 1)) {
             alive = false;
             break;
           }
+        } else if (stopped(ctl)) {
+          alive = false;
+          break;
         }
-        V up_m = P::shfl_up(M[R - 1]);
-        V up_i = P::shfl_up(I[R - 1]);
-        V up_d = P::shfl_up(D[R - 1]);
-        if (lane == 0) {
-          if (from_ring) {
-            const Cell cell = ring[((s / kWarp) & 1) * kWarp + (s & (kWarp - 1))];
-            up_m = cell.m; up_i = cell.i; up_d = cell.d;
+        const Cell* rc = ring + (k & 1) * kWarp;
+        const int s0 = k * kWarp;
+        const int cnt = nsteps - s0 < kWarp ? nsteps - s0 : kWarp;
+        // four steps per loop iteration (C3's FP64 pass: 10.2 ms at two, 9.3 at four)
+#pragma unroll 4
+        for (int i = 0; i < cnt; ++i) {
+          const int s = s0 + i;
+          const uint32_t cx = cx_next, cy = cy_next;
+          cx_next = hx[s];
+          if (!F::kSameHap) cy_next = hy[s];
+          V e[R], t_last;
+          if constexpr (kTwo) {
+            V in_t = P::shfl_up(h_t), in_i = P::shfl_up(h_i);
+            if (lane == 0) {
+              const Cell cl = rc[i];
+              in_t = cl.t; in_i = cl.i;
+            }
+            F::load_emission(table, lane, cx, cy, e);
+            F::cells_scaled(e, dg_t, in_i, M, I, D, pr, t_last);
+            dg_t = in_t;
+            h_t = P::fma(pr.mmU, M[R - 1], P::add(I[R - 1], D[R - 1]));
+            h_i = P::fma(pr.iiN, I[R - 1], M[R - 1]);
+            if (store) dst[s] = Cell{h_t, h_i};
           } else {
-            up_m = P::zero(); up_i = P::zero(); up_d = init;
-          }
-        }
-        V e[R], t_last;
-        F::load_emission(table, lane, cx, cy, e);
-        F::cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr, t_last);
-        if (!last && lane == kWarp - 1) {
-          const int col = s - (kWarp - 1) + 1;
-          if (col >= 1 && col <= (int)H) {
-            Cell cell;
-            cell.m = M[R - 1]; cell.i = I[R - 1]; cell.d = D[R - 1];
-            dst[col] = cell;
-            if (publish && ((col & (kWarp - 1)) == 0 || col == (int)H)) {
-              __threadfence_block();
-              st_release_cta(&ctl.prog[out_row], enc(p, (uint32_t)col));
+            V up_m = P::shfl_up(M[R - 1]);
+            V up_i = P::shfl_up(I[R - 1]);
+            V up_d = P::shfl_up(D[R - 1]);
+            if (lane == 0) {
+              const Cell cl = rc[i];
+              up_m = cl.m; up_i = cl.i; up_d = cl.d;
+            }
+            F::load_emission(table, lane, cx, cy, e);
+            F::cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr, t_last);
+            if (store) {
+              Cell cl;
+              cl.m = M[R - 1]; cl.i = I[R - 1]; cl.d = D[R - 1];
+              dst[s] = cl;
             }
           }
+          (void)t_last;
+          if (last) {
+            acc = P::add(acc, I[R - 1]);
+            if (P::kSlots == 2 && !F::kSameHap && s == nfreeze - 1) frozen = P::sy(acc);
+          }
         }
-        if (last) {
-          acc_m = P::fma(t_last, e[R - 1], acc_m);  // += M[R-1], one rounding
-          acc_i = P::add(acc_i, I[R - 1]);
-          if (P::kSlots == 2 && !F::kSameHap && s == nfreeze - 1) {
-            frozen_m = P::sy(acc_m);
-            frozen_i = P::sy(acc_i);
+        if (store && publish) {
+          // columns up to (the chunk's last step) - 30 are stored
+          const int col = s0 + cnt - 1 - (kWarp - 2);
+          if (col >= 1) {
+            __threadfence_block();
+            st_release_cta(&ctl.prog[out_row], enc(p, (uint32_t)col));
           }
         }
       }
@@ -262,14 +373,12 @@ struct PipeForward {
       }
       if (!alive) break;
       if (last) {
-        out.acc_m = acc_m;
-        out.acc_i = acc_i;
-        out.frozen_m = frozen_m;
-        out.frozen_i = frozen_i;
+        out.acc = acc;
+        out.frozen = frozen;
       } else if constexpr (P::kSlots == 2) {
         __syncwarp();  // lane 31's row stores are visible to the whole warp
         const uint32_t Hs[2] = {sl[0].H, sl[1].H};
-        if (F::row_bound_rejects(b, c, dst, Hs, L, (p + 1) * (kWarp * R) - 1, lane, item)) {
+        if (rejects(b, c, out_cells, Hs, L, (p + 1) * (kWarp * R) - 1, lane, item)) {
           if (lane == 0) atomicCAS(&ctl.stop, 0u, kStopRejected);
           break;
         }
@@ -296,26 +405,20 @@ struct PipeForward {
       return;
     }
     if (warp != (int)((sm.passes - 1) % W) || lane != kWarp - 1) return;
-    S fm = sm.frozen_m, fi = sm.frozen_i;
-    if (P::kSlots == 2 && F::kSameHap) {  // both slots ran exactly their own columns
-      fm = P::sy(sm.acc_m);
-      fi = P::sy(sm.acc_i);
-    }
+    // both slots of a same-haplotype item ran exactly their own columns
+    const S fy = (P::kSlots == 2 && F::kSameHap) ? P::sy(sm.acc) : sm.frozen;
     const uint32_t Lx = b.reads[fr[0].read].len;
     const uint32_t Ly = valid_y ? b.reads[fr[1].read].len : 0u;
     const uint32_t rows = sm.passes * kWarp * R;
     double res[2] = {0.0, 0.0};
     double amin[2] = {(double)kMinAcceptedF, (double)kMinAcceptedF};
     if (F::kScaled) {
-      res[0] = F::scaled_result(b, fr[0].read, Lx, rows, P::sx(sm.acc_m), P::sx(sm.acc_i),
-                                &amin[0]);
-      if (valid_y) res[1] = F::scaled_result(b, fr[1].read, Ly, rows, fm, fi, &amin[1]);
-    } else if (UNIFORM) {
-      res[0] = F::uniform_gapm(b, fr[0].read) * P::sx(sm.acc_m) + P::sx(sm.acc_i);
-      if (valid_y) res[1] = F::uniform_gapm(b, fr[1].read) * fm + fi;
+      res[0] = F::scaled_result(b, fr[0].read, Lx, rows, S(0), P::sx(sm.acc), &amin[0]);
+      if (valid_y) res[1] = F::scaled_result(b, fr[1].read, Ly, rows, S(0), fy, &amin[1]);
     } else {
-      res[0] = P::sx(sm.acc_m) + P::sx(sm.acc_i);
-      res[1] = fm + fi;
+      // the pass-through row holds M_L + I_L in its I (non-uniform form)
+      res[0] = P::sx(sm.acc);
+      res[1] = fy;
     }
     F::finish(b, c, fr[0], res[0], amin[0]);
     if (valid_y) F::finish(b, c, fr[1], res[1], amin[1]);
