@@ -40,6 +40,7 @@ Service::~Service() {
     std::lock_guard<std::mutex> lk(mu_);
     stop_ = true;
   }
+  if (ring_) ring_->stop();
   cv_work_.notify_all();
   cv_space_.notify_all();
   cv_done_.notify_all();
@@ -79,6 +80,10 @@ rodv_status Service::init() {
   slot_budget_ = budget / kSlots;
   batch_bytes_ = std::min<uint64_t>(slot_budget_, kBatchBytes);
   max_inflight_ = opt_.max_inflight ? opt_.max_inflight : 4096;
+  // Each of the ring's five arrays holds about a batch's bases (a batch's
+  // device estimate counts 4 bytes per read base); requests above half of it
+  // keep their own copy.
+  ring_.reset(new HostRing(std::max<uint64_t>(batch_bytes_, 1ull << 20)));
   for (Slot& s : slots_) {
     // staging holds at most the estimate; results are 8 of its ~36 bytes per pair
     if (e == cudaSuccess) e = s.staging.ensure(batch_bytes_);
@@ -137,29 +142,49 @@ rodv_status Service::submit(const rodv_batch& b, uint64_t* ticket) {
     return refuse(RODV_ERR_ADMISSION, "request needs ~" + std::to_string(r->bytes) +
                                           " device bytes; a batch slot holds " +
                                           std::to_string(slot_budget_));
-  // owned copy, haplotypes and reads rebased to contiguous arrays
+  // Copy of the bases and qualities: into the ring when the request fits in
+  // half of it (haplotypes, then reads, at the same position in every
+  // array), else into the request's own arrays.
   uint64_t hb = 0, rb = 0;
   for (uint32_t h = 0; h < b.num_haps; ++h) hb += b.hap_lengths[h];
   for (uint32_t k = 0; k < b.num_reads; ++k) rb += b.read_lengths[k];
-  r->hap_bases.resize(hb);
+  r->hap_bytes = hb;
+  r->read_bytes = rb;
   r->hap_off.resize(b.num_haps);
   r->hap_len.assign(b.hap_lengths, b.hap_lengths + b.num_haps);
-  for (uint64_t h = 0, o = 0; h < b.num_haps; ++h) {
-    std::memcpy(r->hap_bases.data() + o, b.hap_bases + b.hap_offsets[h], b.hap_lengths[h]);
-    r->hap_off[h] = o;
-    o += b.hap_lengths[h];
-  }
-  r->read_bases.resize(rb);
-  for (auto& q : r->quals) q.resize(rb);
   r->read_off.resize(b.num_reads);
   r->read_len.assign(b.read_lengths, b.read_lengths + b.num_reads);
-  const uint8_t* src_q[4] = {b.base_quals, b.ins_quals, b.del_quals, b.gcp_quals};
+  uint8_t* hap_dst;
+  uint8_t* read_dst[HostRing::kArrays];
+  uint64_t hap_base = 0, read_base = 0;  // offsets of the copies in their arrays
+  if (hb + rb <= ring_->capacity() / 2) {
+    const uint64_t pos = ring_->acquire(hb + rb);
+    if (pos == HostRing::kNone) return RODV_ERR_SHUTDOWN;
+    r->ring_pos = pos;
+    hap_base = pos;
+    read_base = pos + hb;
+    hap_dst = ring_->array(0) + hap_base;
+    for (int k = 0; k < HostRing::kArrays; ++k) read_dst[k] = ring_->array(k) + read_base;
+  } else {
+    r->hap_bases.resize(hb);
+    r->read_bases.resize(rb);
+    for (auto& q : r->quals) q.resize(rb);
+    hap_dst = r->hap_bases.data();
+    read_dst[0] = r->read_bases.data();
+    for (int q = 0; q < 4; ++q) read_dst[q + 1] = r->quals[q].data();
+  }
+  for (uint64_t h = 0, o = 0; h < b.num_haps; ++h) {
+    std::memcpy(hap_dst + o, b.hap_bases + b.hap_offsets[h], b.hap_lengths[h]);
+    r->hap_off[h] = hap_base + o;
+    o += b.hap_lengths[h];
+  }
+  const uint8_t* src[HostRing::kArrays] = {b.read_bases, b.base_quals, b.ins_quals, b.del_quals,
+                                           b.gcp_quals};
   for (uint64_t k = 0, o = 0; k < b.num_reads; ++k) {
     const uint64_t off = b.read_offsets[k];
     const uint32_t n = b.read_lengths[k];
-    std::memcpy(r->read_bases.data() + o, b.read_bases + off, n);
-    for (int q = 0; q < 4; ++q) std::memcpy(r->quals[q].data() + o, src_q[q] + off, n);
-    r->read_off[k] = o;
+    for (int a = 0; a < HostRing::kArrays; ++a) std::memcpy(read_dst[a] + o, src[a] + off, n);
+    r->read_off[k] = read_base + o;
     o += n;
   }
   r->regions.assign(b.regions, b.regions + b.num_regions);
@@ -172,7 +197,11 @@ rodv_status Service::submit(const rodv_batch& b, uint64_t* ticket) {
   {
     std::unique_lock<std::mutex> lk(mu_);
     cv_space_.wait(lk, [&] { return stop_ || inflight_ < max_inflight_; });
-    if (stop_) return RODV_ERR_SHUTDOWN;
+    if (stop_) {
+      lk.unlock();
+      if (r->ring_pos != HostRing::kNone) ring_->release(r->ring_pos);
+      return RODV_ERR_SHUTDOWN;
+    }
     r->ticket = next_ticket_++;
     r->submitted = Clock::now();
     if (!st_any_) {
@@ -230,6 +259,7 @@ void Service::worker() {
       s.batch_id = next_batch_++;
       const Clock::time_point t0 = Clock::now();
       const rodv_status st = launch(s);
+      release_ring(s);  // packed into the slot's staging: the ring ranges are free
       {
         std::lock_guard<std::mutex> lk(mu_);
         st_launch_ms_ += ms_between(t0, Clock::now());
@@ -254,34 +284,41 @@ void Service::worker() {
 rodv_status Service::launch(Slot& s) {
   TraceRange trace("rodv service: form and launch batch");
   const Clock::time_point t0 = Clock::now();
-  // The combined batch: requests' regions, haplotypes and reads back to back,
-  // in the slot's arrays (resized below; every element is overwritten).
-  // Each request's arrays go to offsets known in advance, so the copies run
-  // on the worker pool (one serial copy of every batch's bases and qualities
-  // took a large share of the worker's time at saturation).
+  // The combined batch: the requests' regions, haplotype and read tables
+  // back to back in the slot's arrays (resized below; every element is
+  // overwritten).  When every request's bases are in the ring (the usual
+  // case), the batch's base and quality arrays are the ring's and its offsets
+  // the requests' ring positions: no base is copied.  Otherwise the bases go
+  // to the slot's arrays too.  Each request's part goes to offsets known in
+  // advance, so the copies run on the worker pool.
   struct Off {
     uint64_t reg, hap, read, hb, rb;
   };
   std::vector<Off> offs(s.reqs.size() + 1);
   uint64_t est = 0;
+  bool in_ring = true;
   for (size_t k = 0; k < s.reqs.size(); ++k) {
     const auto& r = s.reqs[k];
     r->started = t0;
     est += r->bytes;
+    in_ring = in_ring && r->ring_pos != HostRing::kNone;
     offs[k + 1] = Off{offs[k].reg + r->regions.size(), offs[k].hap + r->hap_len.size(),
-                      offs[k].read + r->read_len.size(), offs[k].hb + r->hap_bases.size(),
-                      offs[k].rb + r->read_bases.size()};
+                      offs[k].read + r->read_len.size(), offs[k].hb + r->hap_bytes,
+                      offs[k].rb + r->read_bytes};
   }
   const Off& tot = offs.back();
   s.regions.resize(tot.reg);
-  s.hap_bases.resize(tot.hb);
-  s.read_bases.resize(tot.rb);
-  for (auto& q : s.quals) q.resize(tot.rb);
+  if (!in_ring) {
+    s.hap_bases.resize(tot.hb);
+    s.read_bases.resize(tot.rb);
+    for (auto& q : s.quals) q.resize(tot.rb);
+  }
   s.hap_off.resize(tot.hap);
   s.read_off.resize(tot.read);
   s.hap_len.resize(tot.hap);
   s.read_len.resize(tot.read);
-  parallel_for(s.reqs.size(), 1, [&](size_t lo, size_t hi) {
+  const size_t grain = in_ring ? 64 : 1;
+  parallel_for(s.reqs.size(), grain, [&](size_t lo, size_t hi) {
     for (size_t k = lo; k < hi; ++k) {
       const Request& r = *s.reqs[k];
       const Off& o = offs[k];
@@ -291,23 +328,47 @@ rodv_status Service::launch(Slot& s) {
         rg.read_start += (uint32_t)o.read;
         s.regions[o.reg + g] = rg;
       }
-      std::memcpy(s.hap_bases.data() + o.hb, r.hap_bases.data(), r.hap_bases.size());
-      std::memcpy(s.read_bases.data() + o.rb, r.read_bases.data(), r.read_bases.size());
-      for (int q = 0; q < 4; ++q)
-        std::memcpy(s.quals[q].data() + o.rb, r.quals[q].data(), r.quals[q].size());
-      for (size_t h = 0; h < r.hap_off.size(); ++h) s.hap_off[o.hap + h] = r.hap_off[h] + o.hb;
-      for (size_t j = 0; j < r.read_off.size(); ++j)
-        s.read_off[o.read + j] = r.read_off[j] + o.rb;
       std::memcpy(s.hap_len.data() + o.hap, r.hap_len.data(), r.hap_len.size() * 4);
       std::memcpy(s.read_len.data() + o.read, r.read_len.data(), r.read_len.size() * 4);
+      if (in_ring) {
+        std::memcpy(s.hap_off.data() + o.hap, r.hap_off.data(), r.hap_off.size() * 8);
+        std::memcpy(s.read_off.data() + o.read, r.read_off.data(), r.read_off.size() * 8);
+        continue;
+      }
+      // the request's bases, wherever submit put them, to the slot's arrays
+      const bool ring = r.ring_pos != HostRing::kNone;
+      const uint64_t hap_base = ring ? r.ring_pos : 0, read_base = hap_base + (ring ? r.hap_bytes : 0);
+      const uint8_t* hsrc = ring ? ring_->array(0) + hap_base : r.hap_bases.data();
+      const uint8_t* rsrc[HostRing::kArrays] = {
+          ring ? ring_->array(0) + read_base : r.read_bases.data(),
+          ring ? ring_->array(1) + read_base : r.quals[0].data(),
+          ring ? ring_->array(2) + read_base : r.quals[1].data(),
+          ring ? ring_->array(3) + read_base : r.quals[2].data(),
+          ring ? ring_->array(4) + read_base : r.quals[3].data()};
+      uint8_t* rdst[HostRing::kArrays] = {s.read_bases.data(), s.quals[0].data(), s.quals[1].data(),
+                                          s.quals[2].data(), s.quals[3].data()};
+      std::memcpy(s.hap_bases.data() + o.hb, hsrc, r.hap_bytes);
+      for (int a = 0; a < HostRing::kArrays; ++a) std::memcpy(rdst[a] + o.rb, rsrc[a], r.read_bytes);
+      for (size_t h = 0; h < r.hap_off.size(); ++h)
+        s.hap_off[o.hap + h] = r.hap_off[h] - hap_base + o.hb;
+      for (size_t j = 0; j < r.read_off.size(); ++j)
+        s.read_off[o.read + j] = r.read_off[j] - read_base + o.rb;
     }
   });
   const Clock::time_point t_comb = Clock::now();
+  const uint8_t* arr[HostRing::kArrays + 1];
+  if (in_ring) {
+    arr[0] = ring_->array(0);
+    for (int a = 0; a < HostRing::kArrays; ++a) arr[a + 1] = ring_->array(a);
+  } else {
+    arr[0] = s.hap_bases.data();
+    arr[1] = s.read_bases.data();
+    for (int q = 0; q < 4; ++q) arr[q + 2] = s.quals[q].data();
+  }
   const rodv_batch b{(uint32_t)s.regions.size(), s.regions.data(), (uint32_t)s.hap_len.size(),
-                     s.hap_bases.data(), s.hap_off.data(), s.hap_len.data(),
-                     (uint32_t)s.read_len.size(), s.read_bases.data(), s.quals[0].data(),
-                     s.quals[1].data(), s.quals[2].data(), s.quals[3].data(),
-                     s.read_off.data(), s.read_len.data()};
+                     arr[0], s.hap_off.data(), s.hap_len.data(), (uint32_t)s.read_len.size(),
+                     arr[1], arr[2], arr[3], arr[4], arr[5], s.read_off.data(),
+                     s.read_len.data()};
   // Buffers grow with headroom: reallocating device or pinned memory
   // synchronises the device, which would stall the other slot's batch.
   {
@@ -407,6 +468,14 @@ void Service::complete(Slot& s) {
   s.reqs.clear();
   cv_done_.notify_all();
   cv_space_.notify_all();
+}
+
+void Service::release_ring(Slot& s) {
+  for (const auto& r : s.reqs)
+    if (r->ring_pos != HostRing::kNone) {
+      ring_->release(r->ring_pos);
+      r->ring_pos = HostRing::kNone;
+    }
 }
 
 void Service::fail_slot(Slot& s, rodv_status st) {

@@ -5,6 +5,9 @@
 // while the GPU was busy into the next device batch (continuous batching) on
 // kSlots slots, each with its own stream, pinned staging and device arena, so
 // the host packs and uploads the next batches while earlier ones compute.
+// Submit copies a request's bases and qualities into the service's host ring
+// (host_ring.h), so forming a batch copies no bases: the batch's arrays are
+// the ring's, and the packer reads each request where submit put it.
 // Admission: a request larger than a slot's share of the device-memory
 // budget is refused (RODV_ERR_ADMISSION); submit blocks while max_inflight
 // requests are queued or running.  A batch takes queued requests up to a
@@ -22,6 +25,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "host_ring.h"
 
 namespace rodv {
 
@@ -41,10 +45,14 @@ class Service {
   using Clock = std::chrono::steady_clock;
   struct Request {
     uint64_t ticket = 0;
-    // owned copy of the caller's regions, rebased to the request's arrays
+    // copy of the caller's regions: bases and qualities in the service's
+    // ring (ring_pos != kNone; hap_off and read_off are ring positions) or,
+    // for a request too large for it, in the request's own arrays
     std::vector<rodv_region> regions;
+    uint64_t ring_pos = HostRing::kNone;
     std::vector<uint8_t> hap_bases, read_bases, quals[4];
     std::vector<uint64_t> hap_off, read_off;
+    uint64_t hap_bytes = 0, read_bytes = 0;
     std::vector<uint32_t> hap_len, read_len;
     uint64_t pairs = 0, cells = 0, bytes = 0;
     Clock::time_point submitted, started, finished;
@@ -75,6 +83,7 @@ class Service {
   rodv_status launch(Slot& s);
   void complete(Slot& s);
   void fail_slot(Slot& s, rodv_status st);
+  void release_ring(Slot& s);
   uint64_t estimate_bytes(const rodv_batch& b, uint64_t pairs) const;
 
   rodv_options opt_;
@@ -84,6 +93,7 @@ class Service {
   uint64_t slot_budget_ = 0;   // largest request (device bytes) a slot admits
   uint64_t batch_bytes_ = 0;   // batches are formed up to this size
   uint32_t max_inflight_ = 0;
+  std::unique_ptr<HostRing> ring_;
 
   std::mutex mu_;
   std::condition_variable cv_work_, cv_done_, cv_space_;
