@@ -222,6 +222,17 @@ void Service::worker() {
   cudaSetDevice(engine_.device_);
   std::deque<int> busy;  // slots with a batch in flight, oldest first
   for (;;) {
+    // Collect every batch that is done, in whatever order they finish (a
+    // small batch launched after a large one often finishes first, and its
+    // slot is then free for what queued meanwhile).
+    for (auto it = busy.begin(); it != busy.end();) {
+      if (cudaEventQuery(slots_[*it].done) != cudaErrorNotReady) {
+        complete(slots_[*it]);
+        it = busy.erase(it);
+      } else {
+        ++it;
+      }
+    }
     int slot = -1;
     std::vector<std::shared_ptr<Request>> batch;
     {
@@ -243,40 +254,31 @@ void Service::worker() {
           batch.push_back(r);
           pending_.pop_front();
         }
-      } else if (!busy.empty() && busy.size() < (size_t)kSlots && pending_.empty()) {
-        // A slot free and nothing queued: launch a new batch as soon as
-        // something arrives, collect the oldest running one when it is done.
-        if (cudaEventQuery(slots_[busy.front()].done) == cudaErrorNotReady) {
-          cv_work_.wait_for(lk, std::chrono::microseconds(200),
-                            [&] { return stop_ || !pending_.empty(); });
-          continue;
-        }
-      }
-    }
-    if (slot >= 0) {
-      Slot& s = slots_[slot];
-      s.reqs = std::move(batch);
-      s.batch_id = next_batch_++;
-      const Clock::time_point t0 = Clock::now();
-      const rodv_status st = launch(s);
-      release_ring(s);  // packed into the slot's staging: the ring ranges are free
-      {
-        std::lock_guard<std::mutex> lk(mu_);
-        st_launch_ms_ += ms_between(t0, Clock::now());
-      }
-      if (st != RODV_OK) {
-        // the slot's stream may still hold part of the batch
-        cudaStreamSynchronize(s.stream);
-        fail_slot(s, st);
       } else {
-        busy.push_back(slot);
+        // Batches in flight, and no slot free or nothing queued: look again
+        // in 50 us, or as soon as something arrives while a slot is free.
+        const bool can_launch = busy.size() < (size_t)kSlots;
+        cv_work_.wait_for(lk, std::chrono::microseconds(50),
+                          [&] { return can_launch && !pending_.empty(); });
+        continue;
       }
-      continue;
     }
-    if (!busy.empty()) {
-      const int i = busy.front();
-      busy.pop_front();
-      complete(slots_[i]);
+    Slot& s = slots_[slot];
+    s.reqs = std::move(batch);
+    s.batch_id = next_batch_++;
+    const Clock::time_point t0 = Clock::now();
+    const rodv_status st = launch(s);
+    release_ring(s);  // packed into the slot's staging: the ring ranges are free
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      st_launch_ms_ += ms_between(t0, Clock::now());
+    }
+    if (st != RODV_OK) {
+      // the slot's stream may still hold part of the batch
+      cudaStreamSynchronize(s.stream);
+      fail_slot(s, st);
+    } else {
+      busy.push_back(slot);
     }
   }
 }
