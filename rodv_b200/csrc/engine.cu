@@ -404,6 +404,25 @@ rodv_status validate_batch(const rodv_batch& b, bool check_bases, uint64_t* num_
   return RODV_OK;
 }
 
+namespace {
+
+// Whether every byte of p[0, n) has low 7 bits v (a quality array of one
+// value), eight bytes at a time.
+bool low7_all_equal(const uint8_t* p, uint32_t n, uint8_t v) {
+  const uint64_t pat = 0x0101010101010101ull * v, mask = 0x7f7f7f7f7f7f7f7full;
+  uint32_t k = 0;
+  for (; k + 8 <= n; k += 8) {
+    uint64_t w;
+    std::memcpy(&w, p + k, 8);
+    if ((w & mask) != pat) return false;
+  }
+  for (; k < n; ++k)
+    if ((p[k] & 127) != v) return false;
+  return true;
+}
+
+}  // namespace
+
 rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64,
                          bool raw) {
   TraceRange trace("rodv: pack");
@@ -458,16 +477,15 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   std::vector<uint8_t>& read_class = plan.read_class;
   read_class.resize(b.num_reads);
   const HostPriorTables& pt = host_prior_tables();
-  parallel_for(b.num_reads, 4096, [&](size_t lo, size_t hi) {
+  parallel_for(b.num_reads, 512, [&](size_t lo, size_t hi) {
     for (size_t r = lo; r < hi; ++r) {
       const uint64_t off = b.read_offsets[r];
       const uint32_t n = b.read_lengths[r];
       const uint8_t i0 = b.ins_quals[off] & 127, d0 = b.del_quals[off] & 127,
                     c0 = b.gcp_quals[off] & 127;
-      bool u = true;
-      for (uint32_t k = 1; k < n && u; ++k)
-        u = (b.ins_quals[off + k] & 127) == i0 && (b.del_quals[off + k] & 127) == d0 &&
-            (b.gcp_quals[off + k] & 127) == c0;
+      const bool u = low7_all_equal(b.ins_quals + off, n, i0) &&
+                     low7_all_equal(b.del_quals + off, n, d0) &&
+                     low7_all_equal(b.gcp_quals + off, n, c0);
       // Uniform-gap classes: ins, del and gcp constant, ins == del (the
       // single-pass kernels' scaled form needs mi == md), gcp quality not 0
       // (gapm = 0), and c = mi*gapm >= 1e-6, so that M/gapm*c -- which the
@@ -521,7 +539,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   std::vector<uint32_t> left_read((size_t)G * 2, kNoPair);
   // single-pass leftover: the odd last read of the region's sorted single-pass reads
   std::vector<uint32_t> single_read(G, kNoPair);
-  parallel_for(G, 64, [&](size_t lo, size_t hi) {
+  parallel_for(G, 16, [&](size_t lo, size_t hi) {
     std::vector<uint32_t> sr;
     for (size_t g = lo; g < hi; ++g) {
       const rodv_region& rg = b.regions[g];
@@ -693,7 +711,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   std::atomic<int> bad_base{-1};
   uint8_t* codes = s + plan.off_hap_codes;
   HapDesc* hd = reinterpret_cast<HapDesc*>(s + plan.off_haps);
-  parallel_for(b.num_haps, 256, [&](size_t lo, size_t hi) {
+  parallel_for(b.num_haps, 64, [&](size_t lo, size_t hi) {
     for (size_t h = lo; h < hi; ++h) {
       const uint8_t* src = b.hap_bases + b.hap_offsets[h];
       uint8_t* dst = codes + hap_code_off[h];
@@ -715,16 +733,29 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   // ---- read rows ----
   uint32_t* rw = reinterpret_cast<uint32_t*>(s + plan.off_read_rows);
   ReadDesc* rdesc = reinterpret_cast<ReadDesc*>(s + plan.off_reads);
-  parallel_for(b.num_reads, 1024, [&](size_t lo, size_t hi) {
+  parallel_for(b.num_reads, 256, [&](size_t lo, size_t hi) {
     for (size_t r = lo; r < hi; ++r) {
       const uint64_t off = b.read_offsets[r];
       const uint32_t n = b.read_lengths[r];
       uint32_t* dst = rw + row_off[r];
-      for (uint32_t k = 0; k < n; ++k) {
-        const uint8_t c = kCodes.v[b.read_bases[off + k]];
-        if (c == 0xff) bad_base.store((int)b.read_bases[off + k]);
-        dst[k] = row_word(c, b.base_quals[off + k], b.ins_quals[off + k], b.del_quals[off + k],
-                          b.gcp_quals[off + k]);
+      const uint8_t* base = b.read_bases + off;
+      const uint8_t* q = b.base_quals + off;
+      if (read_class[r] & 1) {
+        // uniform gaps: insertion, deletion and gcp qualities are the same
+        // on every row, so their fields are one constant
+        const uint32_t gaps = row_word(0, 0, b.ins_quals[off], b.del_quals[off], b.gcp_quals[off]);
+        for (uint32_t k = 0; k < n; ++k) {
+          const uint8_t c = kCodes.v[base[k]];
+          if (c == 0xff) bad_base.store((int)base[k]);
+          dst[k] = gaps | (c & 7u) | ((uint32_t)(q[k] & 127) << 3);
+        }
+      } else {
+        for (uint32_t k = 0; k < n; ++k) {
+          const uint8_t c = kCodes.v[base[k]];
+          if (c == 0xff) bad_base.store((int)base[k]);
+          dst[k] = row_word(c, q[k], b.ins_quals[off + k], b.del_quals[off + k],
+                            b.gcp_quals[off + k]);
+        }
       }
       for (uint32_t k = n; k < ((n + 3) & ~3u); ++k) dst[k] = 0;
       rdesc[r].row_off = row_off[r];
@@ -751,7 +782,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   }
   std::vector<PairRef> leftovers[kNumClasses];
   for (int c = 0; c < kNumClasses; ++c) leftovers[c].resize(left_tot[c]);
-  parallel_for(G, 64, [&](size_t lo, size_t hi) {
+  parallel_for(G, 16, [&](size_t lo, size_t hi) {
     std::vector<uint32_t> byclass[kNumClasses];
     std::vector<uint32_t> sr;
     for (size_t g = lo; g < hi; ++g) {

@@ -393,8 +393,18 @@ rodv_status Service::launch(Slot& s) {
   uint8_t* h = static_cast<uint8_t*>(s.out_host.ptr);
   e = cudaMemcpyAsync(d, s.staging.ptr, p.upload_bytes, cudaMemcpyHostToDevice, s.stream);
   if (e != cudaSuccess) return engine_.cuda_fail(e, "service upload");
-  st = engine_.launch_all(p, d, nullptr, s.stream, s.ev, 3);
+  // Batches compute one after the other: this batch's kernels wait for the
+  // previous batch's (its upload overlaps them), and its classes run as
+  // parallel branches, whose tails overlap.  Run side by side, the batches in
+  // flight shared the GPU and each took about as long as all of them
+  // together, which is what a request waited for.
+  if (prev_kernels_) {
+    e = cudaStreamWaitEvent(s.stream, prev_kernels_, 0);
+    if (e != cudaSuccess) return engine_.cuda_fail(e, "service batch order");
+  }
+  st = engine_.launch_all(p, d, nullptr, s.stream, s.ev, 3, /*fan_out=*/true);
   if (st != RODV_OK) return st;
+  prev_kernels_ = s.ev[2];
   e = cudaMemcpyAsync(h, d + p.off_out, p.num_pairs * 8, cudaMemcpyDeviceToHost, s.stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(h + p.num_pairs * 8, d + p.off_counts, kCountWords * 4,

@@ -93,6 +93,7 @@ class Service {
   uint64_t slot_budget_ = 0;   // largest request (device bytes) a slot admits
   uint64_t batch_bytes_ = 0;   // batches are formed up to this size
   uint32_t max_inflight_ = 0;
+  cudaEvent_t prev_kernels_ = nullptr;  // end of the last launched batch's kernels
   std::unique_ptr<HostRing> ring_;
 
   std::mutex mu_;
