@@ -639,7 +639,9 @@ struct Forward {
       sl[s].row_off = rd.row_off;
     }
     const uint32_t Lmax = sl[0].L > sl[1].L ? sl[0].L : sl[1].L;
-    const uint32_t passes = MULTI ? (Lmax + kWarp * R - 1) / (kWarp * R) : 1;
+    // (pipe_passes: the last pass ends in pass-through rows, as in the
+    // pipelined sweep, so both give the same results)
+    const uint32_t passes = MULTI ? pipe_passes(Lmax, R) : 1;
     if (sl[0].H == 0 || sl[1].H == 0 || sl[0].L == 0 || sl[1].L == 0 ||
         (kSameHap && sl[0].hap != sl[1].hap) || (!MULTI && Lmax > (uint32_t)(kWarp * R)) ||
         (MULTI && (uint64_t)sl[0].H + 40 > c.scratch_cols)) {

@@ -100,6 +100,11 @@ struct PipeForward {
   static_assert(sizeof(Cell) <= 24, "the engine sizes boundary rows at 24 bytes a cell");
   static constexpr int kRows = W + 1;                   // boundary rows per block
   static constexpr int kPad = kWarp;                    // cells before column 0 of a row
+  // Steps per loop iteration.  FP32: four (C3's FP32 pass 2.78 ms, 3.09 at
+  // two).  FP64: two, 166 registers at R = 8, so three warps a sub-partition
+  // (C3's FP64 pass 7.19 ms; 7.33 at four, 173 registers and two warps; 8.25
+  // at one; 9.76 at one capped to 128 registers and four warps).
+  static constexpr int kUnroll = P::kSlots == 1 ? 2 : 4;
   static constexpr int kSmemPerWarp = F::kSmemPerWarp;  // emission table + cell ring
   // polls of a progress word (about 100 ns each) before a wait gives up
   static constexpr uint32_t kWaitPolls = 1u << 24;
@@ -316,8 +321,7 @@ struct PipeForward {
         const Cell* rc = ring + (k & 1) * kWarp;
         const int s0 = k * kWarp;
         const int cnt = nsteps - s0 < kWarp ? nsteps - s0 : kWarp;
-        // four steps per loop iteration (C3's FP64 pass: 10.2 ms at two, 9.3 at four)
-#pragma unroll 4
+#pragma unroll kUnroll
         for (int i = 0; i < cnt; ++i) {
           const int s = s0 + i;
           const uint32_t cx = cx_next, cy = cy_next;
