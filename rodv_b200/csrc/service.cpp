@@ -233,13 +233,21 @@ void Service::worker() {
         ++it;
       }
     }
+    // A new batch is formed only once every batch in flight has started on
+    // the GPU: at most one batch waits behind the running one, and what
+    // arrives meanwhile goes into the next batch instead of one queued two
+    // batches ahead.
+    bool all_started = true;
+    for (int i : busy)
+      all_started = all_started && cudaEventQuery(slots_[i].ev[0]) != cudaErrorNotReady;
+    const bool can_launch = busy.size() < (size_t)kSlots && all_started;
     int slot = -1;
     std::vector<std::shared_ptr<Request>> batch;
     {
       std::unique_lock<std::mutex> lk(mu_);
       if (busy.empty()) cv_work_.wait(lk, [&] { return stop_ || !pending_.empty(); });
       if (busy.empty() && pending_.empty() && stop_) break;
-      if (busy.size() < (size_t)kSlots && !pending_.empty()) {
+      if (can_launch && !pending_.empty()) {
         // everything queued, up to one batch's size, goes into the next batch
         for (int i = 0; i < kSlots && slot < 0; ++i)
           if (std::find(busy.begin(), busy.end(), i) == busy.end()) slot = i;
@@ -255,9 +263,8 @@ void Service::worker() {
           pending_.pop_front();
         }
       } else {
-        // Batches in flight, and no slot free or nothing queued: look again
-        // in 50 us, or as soon as something arrives while a slot is free.
-        const bool can_launch = busy.size() < (size_t)kSlots;
+        // Batches in flight, and no launch due or nothing queued: look again
+        // in 50 us, or as soon as something arrives while a launch is due.
         cv_work_.wait_for(lk, std::chrono::microseconds(50),
                           [&] { return can_launch && !pending_.empty(); });
         continue;
