@@ -20,7 +20,8 @@ Reported (see the JSON keys):
              this GPU in this run (FMA-chain kernels, rodv_measure_peaks);
              12 algorithmic flops per cell (4 mul + 2 add for M, 2 mul + 1 add
              for I and for D); traffic is the DRAM bytes of those kernels per
-             step from an ncu capture of the full-size workload.
+             step, from an ncu capture of the dominant class's kernel on the
+             same sources (profiles/), scaled to the step by its cell share.
   plain_form the plain GPU form (one launch per pair) against the batched
              engine on the same sample.
   cpu_baseline  the reference's own schedule_pairhmm (oracle/_ref), threads
@@ -61,8 +62,34 @@ KERNEL_SOURCES = ["pairhmm_fwd.cuh", "pairhmm_pipe.cuh", "layout.h", "kernel_tab
                   "kernels.h", "pairhmm_kernels.cu", "kernels_r*.cu", "kernels_multi_r*.cu"]
 
 
+def _code_only(text):
+    """C++ source without its comments and blank or trailing space: what the
+    compiler sees, so that editing a comment keeps a capture valid."""
+    out, i, n = [], 0, len(text)
+    while i < n:
+        c = text[i]
+        if c in "\"'":  # string or character literal, copied whole
+            j = i + 1
+            while j < n and text[j] != c:
+                j += 2 if text[j] == "\\" else 1
+            out.append(text[i:j + 1])
+            i = j + 1
+        elif text.startswith("//", i):
+            j = text.find("\n", i)
+            i = n if j < 0 else j
+        elif text.startswith("/*", i):
+            j = text.find("*/", i + 2)
+            i = n if j < 0 else j + 2
+        else:
+            out.append(c)
+            i += 1
+    lines = (ln.rstrip() for ln in "".join(out).splitlines())
+    return "\n".join(ln for ln in lines if ln)
+
+
 def kernel_source_sha():
-    """sha256 (first 16 hex digits) of the forward kernels' sources."""
+    """sha256 (first 16 hex digits) of the forward kernels' sources, comments
+    and blank lines left out."""
     import glob
     import hashlib
     h = hashlib.sha256()
@@ -70,8 +97,8 @@ def kernel_source_sha():
     names = sorted({os.path.basename(p) for pat in KERNEL_SOURCES
                     for p in glob.glob(os.path.join(csrc, pat))})
     for name in names:
-        with open(os.path.join(csrc, name), "rb") as fh:
-            h.update(name.encode() + b"\0" + fh.read())
+        with open(os.path.join(csrc, name), encoding="utf-8") as fh:
+            h.update(name.encode() + b"\0" + _code_only(fh.read()).encode())
     return h.hexdigest()[:16]
 
 

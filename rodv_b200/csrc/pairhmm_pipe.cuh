@@ -30,10 +30,9 @@
 // waiting for its producer (pass p-1): waits point to strictly earlier
 // passes, so they cannot form a cycle.  Each wait also gives up after a
 // bounded number of polls, sets kErrWaitTimeout and stops the item, so a
-// kernel always ends.  A row starts with kPad cells
-// before its column 0: lane 31 stores its hand-over every step, the first 31
-// of which are columns <= 0 (zeros, never read), so no store needs a column
-// test.
+// kernel always ends.  A row starts with kPad cells before its column 0:
+// lane 31 stores its hand-over every step, the first 31 of which are columns
+// <= 0 (zeros, never read), so no store needs a column test.
 //
 // Progress words live in shared memory: (pass << 17) | column, written with a
 // CTA-scope release by the producing lane after its row stores (and a block
@@ -48,10 +47,11 @@
 // item stops on every warp and both pairs go to FP64.  The bound is exact, so
 // the rescued pairs and every result are those of the full sweep.  (Holding
 // pass 1 back until pass 0's verdict, so that a rejected item costs one pass
-// instead of the passes in flight, made no difference on 2,000 long pairs
-// that all go to FP64, C3: 2.92 ms FP32 pass either way, since the warps of
-// these latency-bound sweeps leave issue slots free; at a quarter of the
-// pairs it was slower, 1.34 against 1.19 ms.)
+// instead of the passes in flight, made no difference on 2,000 pairs of
+// 1,000-2,000-base reads and 2,000-5,000-base haplotypes that all go to FP64
+// (2.92 ms FP32 pass either way, since the warps of these latency-bound
+// sweeps leave issue slots free); at a quarter of the pairs it was slower,
+// 1.34 against 1.19 ms.)
 //
 // Results are committed after a block barrier at the end of the item: by the
 // warp that swept the last pass, or, for a rejected item, as FP64 rescues.
@@ -100,10 +100,11 @@ struct PipeForward {
   static_assert(sizeof(Cell) <= 24, "the engine sizes boundary rows at 24 bytes a cell");
   static constexpr int kRows = W + 1;                   // boundary rows per block
   static constexpr int kPad = kWarp;                    // cells before column 0 of a row
-  // Steps per loop iteration.  FP32: four (C3's FP32 pass 2.78 ms, 3.09 at
-  // two).  FP64: two, 166 registers at R = 8, so three warps a sub-partition
-  // (C3's FP64 pass 7.19 ms; 7.33 at four, 173 registers and two warps; 8.25
-  // at one; 9.76 at one capped to 128 registers and four warps).
+  // Steps per loop iteration, measured on the 2,000 long pairs above.  FP32:
+  // four (FP32 pass 2.78 ms, 3.09 at two).  FP64: two, 166 registers at R = 8,
+  // so three warps a sub-partition (FP64 pass 7.19 ms; 7.33 at four, 173
+  // registers and two warps; 8.25 at one; 9.76 at one capped to 128
+  // registers and four warps).
   static constexpr int kUnroll = P::kSlots == 1 ? 2 : 4;
   static constexpr int kSmemPerWarp = F::kSmemPerWarp;  // emission table + cell ring
   // polls of a progress word (about 100 ns each) before a wait gives up
