@@ -61,3 +61,18 @@ def test_roofline_traffic_comes_from_a_capture_of_these_kernels():
     assert t is not None and 2e8 < t < 5e9, note
     assert bench.step_traffic_bytes("uneven", 0.5)[0] is None
     assert bench.step_traffic_bytes("stream", 1.0)[0] is None
+
+
+def test_kernel_source_hash_ignores_comments_only():
+    """The capture's source hash follows the compiled code: comments, blank
+    lines and trailing spaces do not change it, any code change does, and
+    comment markers inside string literals are code."""
+    sys.path.insert(0, ROOT)
+    import bench
+    a = 'int f() {\n  return 1;  // one\n}\n/* block\n comment */\nconst char* s = "a//b";\n'
+    b = '// new header\nint f() {\n  return 1;\n}\n\nconst char* s = "a//b";   \n'
+    c = 'int f() {\n  return 2;\n}\nconst char* s = "a//b";\n'
+    d = 'int f() {\n  return 1;\n}\nconst char* s = "a";\n'
+    assert bench._code_only(a) == bench._code_only(b)
+    assert bench._code_only(a) != bench._code_only(c)
+    assert bench._code_only(a) != bench._code_only(d)
