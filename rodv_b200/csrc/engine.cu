@@ -325,6 +325,26 @@ rodv_status Engine::init() {
   return RODV_OK;
 }
 
+// Every forward kernel the engine can launch, loaded now: with CUDA's lazy
+// module loading a kernel's first launch loads it, which stalls that launch
+// for milliseconds (the occupancy query both loads it and fills the cache
+// persistent_blocks uses).
+rodv_status Engine::load_kernels() {
+  RODV_CUDA(cudaSetDevice(device_));
+  for (int c = 0; c < kNumClasses; ++c)
+    for (int p = 0; p < 3; ++p) {
+      const Precision pr = p == 2 ? Precision::kF64 : Precision::kF32x2;
+      const int nv = forward_kernel_variants(pr, p == 0, class_rows(c), class_multi(c));
+      for (int v = 0; v < nv; ++v) {
+        const KernelInfo k =
+            forward_kernel_info(pr, class_rows(c), class_uniform(c), class_multi(c), p == 0, v);
+        if (k.fn) persistent_blocks(k);
+      }
+    }
+  RODV_CUDA(cudaGetLastError());
+  return RODV_OK;
+}
+
 // Boundary rows a multi-pass class's kernels need: per block of the largest
 // grid any multi-pass kernel variant launches (the autotuner runs every
 // variant on its batches).

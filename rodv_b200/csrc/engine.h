@@ -118,6 +118,8 @@ class Engine {
   explicit Engine(const rodv_options& opt);
   ~Engine();
   rodv_status init();
+  // Loads every forward kernel variant now instead of at its first launch.
+  rodv_status load_kernels();
 
   // prec: null, or raw mode (rodv_pairhmm_batch_raw): out receives raw
   // likelihoods and prec the precision of each.

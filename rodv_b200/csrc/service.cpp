@@ -61,6 +61,14 @@ rodv_status Service::init() {
     err_ = engine_.last_error();
     return st;
   }
+  // A kernel's first launch would otherwise load it in the middle of a batch
+  // (a stall of milliseconds for every request of that batch and the ones
+  // queued behind it).
+  st = engine_.load_kernels();
+  if (st != RODV_OK) {
+    err_ = engine_.last_error();
+    return st;
+  }
   ready_ = true;  // streams and events created below are released by the destructor
   cudaError_t e = cudaSetDevice(engine_.device_);
   for (Slot& s : slots_) {
@@ -84,6 +92,9 @@ rodv_status Service::init() {
   // device estimate counts 4 bytes per read base); requests above half of it
   // keep their own copy.
   ring_.reset(new HostRing(std::max<uint64_t>(batch_bytes_, 1ull << 20)));
+  // Touched once now, so that no request's copy takes the ring's first-use
+  // page faults.
+  for (int k = 0; k < HostRing::kArrays; ++k) std::memset(ring_->array(k), 0, ring_->capacity());
   for (Slot& s : slots_) {
     // staging holds at most the estimate; results are 8 of its ~36 bytes per pair
     if (e == cudaSuccess) e = s.staging.ensure(batch_bytes_);
