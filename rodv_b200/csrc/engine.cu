@@ -1203,7 +1203,9 @@ rodv_status Engine::run_host_chunked(const rodv_batch& b, double* out, rodv_stat
       result = cuda_fail(e, "chunk upload");
       break;
     }
-    result = launch_all(p, d, &acc, l.stream, l.ev, 3);
+    // the range's classes as parallel branches (their tails overlap; 130 ms
+    // per call of the uneven batch against 132-134 without)
+    result = launch_all(p, d, &acc, l.stream, l.ev, 3, /*fan_out=*/true);
     if (result != RODV_OK) break;
     e = cudaMemcpyAsync(h, d + p.off_out, p.num_pairs * 8, cudaMemcpyDeviceToHost, l.stream);
     if (e == cudaSuccess)
