@@ -165,8 +165,9 @@ class Engine {
   // or three events recorded before the FP32 launches, between the two parts
   // and after the FP64 launches.  fan_out: each class's launches go to its own
   // side stream (forked from and joined back into `stream`), so that class
-  // kernels fill each other's tails; for the captured resident path, whose
-  // engine-owned side streams no other caller uses at the same time.
+  // kernels fill each other's tails.  The side streams are the engine's: the
+  // captured resident path, the host-buffer ranges and the service's batches
+  // use them from the one thread that launches for the engine at a time.
   rodv_status launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stats* st,
                          cudaStream_t stream, cudaEvent_t* ev, int parts,
                          bool fan_out = false);
