@@ -699,8 +699,11 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   }
   const size_t lists_begin = o;
   for (int c = 0; c < kNumClasses; ++c) {
+    plan.list_cap[c] = plan.pairs[c];
+    if (!fp64 && class_multi(c))
+      plan.list_cap[c] = std::max(plan.pairs[c], 2u * (plan.same_items[c] + plan.diff_items[c]));
     plan.off_lists[c] = o;
-    o = align_up(o + (size_t)plan.pairs[c] * sizeof(PairRef));
+    o = align_up(o + (size_t)plan.list_cap[c] * sizeof(PairRef));
   }
   // forced FP64: the lists are full from the start; their lengths are uploaded
   // too and copied into the counters at every run
@@ -914,6 +917,10 @@ rodv_status Engine::launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, in
   cl.scratch = class_scratch(plan, a, c);
   cl.scratch_cols = plan.scratch_cols;
   cl.error_flags = a.counts + kCtrError;
+  if (class_multi(c)) {  // rescues at their items' positions: same items, then two-haplotype
+    cl.flags |= kLaunchRescueByItem;
+    cl.rescue_base = same ? 0u : 2u * plan.same_items[c];
+  }
   apply_wait_fault(cl, c);
   const int per_block = k.items_per_block;
   const int need = (int)((n + per_block - 1) / per_block);
@@ -935,6 +942,12 @@ rodv_status Engine::launch_fp64_class(const PackedPlan& plan, uint8_t* dbase, in
   cl.work = dbase + plan.off_lists[c];
   cl.work_count = a.counts + kCtrRescue + c;
   cl.static_count = 0;
+  if (class_multi(c) && !plan.fp64) {
+    // rescues sit at their FP32 items' positions (longest items first); the
+    // kernel passes over the empty positions
+    cl.work_count = nullptr;
+    cl.static_count = 2u * (plan.same_items[c] + plan.diff_items[c]);
+  }
   cl.counter = a.counts + kCtrF64 + c;
   cl.scratch = class_scratch(plan, a, c);
   cl.scratch_cols = plan.scratch_cols;
@@ -980,6 +993,12 @@ rodv_status Engine::launch_all(const PackedPlan& plan, uint8_t* dbase, rodv_stat
     if (plan.fp64)  // every pair goes to the FP64 kernels: the uploaded lists are full
       RODV_CUDA(cudaMemcpyAsync(a.counts + kCtrRescue, dbase + plan.off_preset,
                                 kNumClasses * 4, cudaMemcpyDeviceToDevice, stream));
+    // multi-pass classes' lists: every position empty (kNoPair) until a
+    // rescue fills it (kLaunchRescueByItem)
+    for (int c = kSinglePassClasses; c < kNumClasses && !plan.fp64; ++c)
+      if (plan.same_items[c] + plan.diff_items[c])
+        RODV_CUDA(cudaMemsetAsync(dbase + plan.off_lists[c], 0xff,
+                                  (size_t)plan.list_cap[c] * sizeof(PairRef), stream));
   }
   if (ev) RODV_CUDA(cudaEventRecord(ev[0], stream));
   if (!plan.fp64 && (parts & 1)) {

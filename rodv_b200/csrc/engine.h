@@ -83,7 +83,10 @@ struct PackedPlan {
   uint32_t chain_haps[kNumClasses] = {};   // haplotypes per chain item (single-pass classes)
   int variant[kNumClasses] = {};           // kernel variant per class the items were packed for
   int variant64[kNumClasses] = {};         // FP64 kernel variant per class
-  uint32_t pairs[kNumClasses] = {};        // pairs per class (FP64 list capacity)
+  uint32_t pairs[kNumClasses] = {};        // pairs per class
+  // FP64 list capacity per class: the pairs, or for a multi-pass class in an
+  // FP32 run two positions per FP32 item (kLaunchRescueByItem)
+  uint32_t list_cap[kNumClasses] = {};
   size_t off_hap_codes = 0, off_read_rows = 0, off_haps = 0, off_reads = 0;
   size_t off_same[kNumClasses] = {};
   size_t off_diff[kNumClasses] = {};

@@ -160,12 +160,19 @@ struct ClassLaunch {
   uint32_t* error_flags;       // bit set by a kernel that hit a bad descriptor
   uint32_t flags;              // kLaunch* bits
   uint32_t wait_polls;         // pipelined sweeps: polls before a wait gives up (0: default)
+  uint32_t rescue_base;        // kLaunchRescueByItem: list position of item 0's first pair
 };
 
 // ClassLaunch::flags.  Testing hook: the producers of a pipelined sweep
 // publish no progress, so every consumer's wait runs out (its expiry path is
 // tested without a fault).
 constexpr uint32_t kLaunchNoPublish = 1u;
+// FP32 multi-pass launches: the rescue of slot s of item i goes to list
+// position rescue_base + 2i + s (the list is cleared to kNoPair entries
+// first) instead of the next free one, so the FP64 sweep takes the rescues in
+// the items' order -- longest first, as packed -- and not in the order the
+// FP32 sweeps rejected them, shortest first.
+constexpr uint32_t kLaunchRescueByItem = 2u;
 
 enum ErrorFlag : uint32_t {
   kErrBadLength = 1u,   // a pair with zero or over-limit length reached a kernel

@@ -961,8 +961,10 @@ struct Forward {
   // result, possibly rescaled in FP64, or an FP64 result).
   // FP32: accepted at >= accept_min (1e-28, the reference's bound, or the
   // scaled form's bound) with an FP64 log10, else queued for FP64.
+  // pos: the pair's list position under kLaunchRescueByItem.
   __device__ static void finish(const BatchView& b, const ClassLaunch& c, const PairRef& ref,
-                                double raw, double accept_min = (double)kMinAcceptedF) {
+                                double raw, double accept_min = (double)kMinAcceptedF,
+                                uint32_t pos = 0) {
     // A likelihood is finite and >= 0; anything else is an arithmetic fault,
     // reported rather than passed on (it would fail the acceptance test and
     // end up as a wrong FP64 value or -inf).
@@ -981,7 +983,7 @@ struct Forward {
         }
       } else {
         const uint32_t k = atomicAdd(c.rescue_count, 1u);
-        c.rescue_list[k] = ref;
+        c.rescue_list[(c.flags & kLaunchRescueByItem) ? pos : k] = ref;
       }
     } else {
       // The reference computes with flush-to-zero on (common.h:58-62), which on

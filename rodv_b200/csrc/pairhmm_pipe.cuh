@@ -205,6 +205,8 @@ struct PipeForward {
     out.ok = false;
     PairRef refs[2];
     F::load_refs(c, item, refs);
+    // an FP64 list position that no rescue filled (kLaunchRescueByItem lists)
+    if (P::kSlots == 1 && refs[0].read == kNoPair) return out;
     SlotInfo sl[2];
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
@@ -402,10 +404,11 @@ struct PipeForward {
     PairRef fr[2];
     F::load_refs(c, item, fr);
     const bool valid_y = P::kSlots == 2 && fr[1].read != kNoPair;
+    const uint32_t pos = c.rescue_base + 2u * item;  // kLaunchRescueByItem positions
     if (stop == kStopRejected) {
       if (warp == 0 && lane == 0) {
-        F::finish(b, c, fr[0], 0.0);
-        if (valid_y) F::finish(b, c, fr[1], 0.0);
+        F::finish(b, c, fr[0], 0.0, (double)kMinAcceptedF, pos);
+        if (valid_y) F::finish(b, c, fr[1], 0.0, (double)kMinAcceptedF, pos + 1);
       }
       return;
     }
@@ -425,8 +428,8 @@ struct PipeForward {
       res[0] = P::sx(sm.acc);
       res[1] = fy;
     }
-    F::finish(b, c, fr[0], res[0], amin[0]);
-    if (valid_y) F::finish(b, c, fr[1], res[1], amin[1]);
+    F::finish(b, c, fr[0], res[0], amin[0], pos);
+    if (valid_y) F::finish(b, c, fr[1], res[1], amin[1], pos + 1);
   }
 };
 
