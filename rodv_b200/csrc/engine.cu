@@ -879,6 +879,24 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       }
       if (n != plan.diff_items[c])
         return fail(RODV_ERR_INTERNAL, "leftover pairing count mismatch");
+      // Multi-pass items go out in decreasing sweep length (passes x columns)
+      // across pass-count groups, so the persistent grids -- and, through the
+      // rescue positions, the FP64 sweep -- take the longest first.
+      if (class_multi(c))
+        std::stable_sort(di, di + n, [&](const DiffItem& x, const DiffItem& y) {
+          return (uint64_t)passes_of(x.x.read) * (b.hap_lengths[x.x.hap] + kWarp) >
+                 (uint64_t)passes_of(y.x.read) * (b.hap_lengths[y.x.hap] + kWarp);
+        });
+    }
+    // the same for the multi-pass classes' same-haplotype items
+    for (int c = kSinglePassClasses; c < kNumClasses; ++c) {
+      SameItem* si = reinterpret_cast<SameItem*>(s + plan.off_same[c]);
+      auto cost = [&](const SameItem& it) {
+        return (uint64_t)std::max(passes_of(it.read_x), passes_of(it.read_y)) *
+               (b.hap_lengths[it.hap] + kWarp);
+      };
+      std::stable_sort(si, si + plan.same_items[c],
+                       [&](const SameItem& x, const SameItem& y) { return cost(x) > cost(y); });
     }
   }
   timer.mark("work");
