@@ -110,6 +110,15 @@ float* class_scratch(const PackedPlan& p, const ArenaView& a, int c) {
                                   (size_t)(c - kSinglePassClasses) * p.scratch_bytes);
 }
 
+// Time per computed cell (lane rows x columns, padding included) of the
+// uniform-gap chain kernels by rows per lane R, relative to R = 8: the
+// autotuner's per-class batches (reads of 32R - 5 bases, one read pair per
+// item) on B200 with each class's fastest variant.  R <= 4 run as two
+// 16-lane items per warp with 2R rows per lane, hence their closeness to
+// R = 8.  The packer places a region's read pairs with it.
+constexpr double kChainCellCost[kMaxRowsPerLane + 1] = {0.0,   1.53,  1.20,  1.09, 1.024,
+                                                        1.093, 1.047, 1.031, 1.0};
+
 // Occupancy variant used before (or without) tuning: the register budget
 // measured best for each rows-per-lane value on B200.
 int default_variant(int cls) {
@@ -304,7 +313,10 @@ rodv_status Engine::init() {
   tab_.mm_d = static_cast<const double*>(put(t.mm_d.data(), kMmTableSize * 8));
   RODV_CUDA(ce);
   // Kernels whose tables exceed the default 48 KB of dynamic shared memory
-  // per block opt in to their size.
+  // per block opt in to their size.  The chain kernels also prefer the
+  // largest shared-memory carveout: with the driver's default split an SM
+  // held 4 blocks of the R = 8 kernel (42 KB each) where 228 KB hold 5, so
+  // the occupancy targets above 4 blocks/SM were not reached.
   for (int c = 0; c < kNumClasses; ++c)
     for (int p = 0; p < 3; ++p)
       for (int v = 0; v < kTuneVariants; ++v) {
@@ -315,6 +327,9 @@ rodv_status Engine::init() {
         if (k.fn && k.smem_bytes > 48 * 1024)
           RODV_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          k.smem_bytes));
+        if (k.fn && k.chain)
+          RODV_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                         (int)cudaSharedmemCarveoutMaxShared));
       }
   ready_ = true;
   if (opt_.tune_cache && opt_.tune_cache[0]) load_tuning(opt_.tune_cache);
@@ -444,7 +459,7 @@ bool low7_all_equal(const uint8_t* p, uint32_t n, uint8_t v) {
 }  // namespace
 
 rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64,
-                         bool raw) {
+                         bool raw, bool stack_uniform) {
   TraceRange trace("rodv: pack");
   PackTimer timer(opt_.verbose >= 2);
   plan = PackedPlan{};
@@ -520,16 +535,20 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
 
   timer.mark("classes");
   // ---- per region and class: reads, chain items, same items, leftovers ----
-  // Single-pass reads of a region are sorted by (uniform gaps, length) and
-  // paired neighbour by neighbour; a pair's class is that of its longer read
-  // (uniform only if both are).  Each pair takes ceil(haps / chain_haps[class])
-  // chain items.  An odd last read is a leftover: its pairs (one per
-  // haplotype) go into two-haplotype items with other regions' leftover
-  // pairs of its class, so that both halves of the f32x2 lanes work (a
-  // one-read chain leaves one half idle; a batch of one-read regions ran at
-  // half the FP32 rate).  Whether a read is a leftover depends on its region
-  // only, and a pair's arithmetic in a two-haplotype item does not depend on
-  // its partner, so results do not depend on the rest of the batch.
+  // Single-pass reads of a region are sorted by (uniform gaps, length).
+  // Reads with per-row gap priors pair neighbour by neighbour, one read per
+  // bin of a chain item, the pair in the class of its longer read (an odd
+  // last one pairs with the shortest uniform read, in a per-row class).
+  // Uniform reads either do the same or, where the cost model below finds it
+  // cheaper, stack into bins of the R = 8 uniform class (stack_uniform).
+  // Each item takes ceil(haps / chain_haps[class]) chain items.  An odd last
+  // read is a leftover: its pairs (one per haplotype) go into two-haplotype
+  // items with other regions' leftover pairs of its class, so that both
+  // halves of the f32x2 lanes work (a one-read chain leaves one half idle; a
+  // batch of one-read regions ran at half the FP32 rate).  Whether a read is
+  // a leftover depends on its region only, and a pair's arithmetic does not
+  // depend on its partner, bin, lanes or kernel, so results do not depend on
+  // the rest of the batch.
   // Multi-pass reads keep their own class: same-haplotype items per
   // haplotype, leftovers in two-haplotype items.
   const uint32_t K = kNumClasses;
@@ -549,10 +568,152 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
     const uint32_t len = std::max(b.read_lengths[x], b.read_lengths[y]);
     return class_of(len, (read_class[x] & 1) && (read_class[y] & 1));
   };
+  // The chain items of a region's sorted single-pass reads sr: per item its
+  // class and read pairs (reads[first, first + 2 * pairs): x, then y or
+  // kNoPair), and the leftover read (kNoPair: none).
+  struct ChainPairs {
+    int cls;
+    uint32_t first, pairs;
+  };
+  struct RegionChains {
+    std::vector<uint32_t> reads;
+    std::vector<ChainPairs> items;
+    uint32_t leftover = kNoPair;
+    std::vector<uint32_t> pair_item;          // stacking scratch: item of each pair
+    std::vector<uint32_t> item_free, item_fill, item_lens;
+    std::vector<int> item_cls;
+    std::vector<uint32_t> bucket[kWarp + 1];
+  };
+  // Lane groups of the uniform classes' chain kernels (the packed variant):
+  // an item holds `lanes` lanes of `rows` rows each (two items of 16 lanes
+  // per warp for the lane-grouped variants).
+  struct ChainGeom {
+    int cls;
+    uint32_t lanes, rows;
+    double cost;  // per item, relative
+  };
+  ChainGeom geom[kMaxRowsPerLane + 1] = {};
+  for (int R = 1; R <= kMaxRowsPerLane; ++R) {
+    const int c = class_of((uint32_t)(R * kWarp) - 1, true);
+    const int ipw = forward_kernel_info(Precision::kF32x2, R, true, false, true, variant_[c])
+                        .items_per_warp;
+    geom[R] = ChainGeom{c, (uint32_t)(kWarp / ipw), (uint32_t)(R * ipw),
+                        R * kChainCellCost[R]};
+  }
+  const ChainGeom& stack_geom = geom[kMaxRowsPerLane];
+  // the cheapest uniform class whose items hold pairs with longer reads of
+  // lengths lens
+  auto cheapest = [&](const uint32_t* lens, size_t n) -> const ChainGeom& {
+    const ChainGeom* best = &stack_geom;
+    for (int R = 1; R < kMaxRowsPerLane; ++R) {
+      uint32_t lanes = 0;
+      for (size_t i = 0; i < n; ++i) lanes += lens[i] / geom[R].rows + 1;
+      if (lanes <= geom[R].lanes && geom[R].cost < best->cost) best = &geom[R];
+    }
+    return *best;
+  };
+  auto region_chains = [&](const std::vector<uint32_t>& sr, RegionChains& rc) {
+    rc.reads.clear();
+    rc.items.clear();
+    rc.leftover = kNoPair;
+    size_t nu = 0;  // reads with per-row gap priors come first
+    while (nu < sr.size() && !(read_class[sr[nu]] & 1)) ++nu;
+    auto add_pair = [&](uint32_t x, uint32_t y) {
+      rc.items.push_back(ChainPairs{pair_class(x, y), (uint32_t)rc.reads.size(), 1});
+      rc.reads.push_back(x);
+      rc.reads.push_back(y);
+    };
+    const size_t m = ((nu & 1) && nu < sr.size()) ? nu + 1 : nu;
+    size_t k = 0;
+    for (; k + 1 < m; k += 2) add_pair(sr[k], sr[k + 1]);
+    if (k < m) {  // odd per-row reads and no uniform one
+      rc.leftover = sr[k];
+      return;
+    }
+    const size_t nU = sr.size() - m;  // uniform reads sr[m..), increasing length
+    if (nU == 0) return;
+    // cost of the one-pair item of a pair whose longer read has `len` bases
+    // (a leftover: half of one)
+    auto pair_cost = [&](uint32_t len) { return cheapest(&len, 1).cost; };
+    double classic = 0.0;
+    for (size_t i = m; i + 1 < sr.size(); i += 2) classic += pair_cost(b.read_lengths[sr[i + 1]]);
+    if (nU & 1) classic += 0.5 * pair_cost(b.read_lengths[sr.back()]);
+    // Stacked: neighbours in decreasing length pair up (the shortest read
+    // of an odd count is the leftover), the pairs go by best fit in that
+    // order into items of the R = 8 class (a pair takes the item with the
+    // fewest free lanes that still holds its len/8 + 1 lanes), and each item
+    // then goes to the cheapest uniform class that holds its pairs.
+    const size_t np = nU / 2;
+    bool stacked = false;
+    double cost = 0.0;
+    if (stack_uniform && np >= 2) {
+      rc.pair_item.assign(np, 0);
+      rc.item_free.clear();
+      for (auto& v : rc.bucket) v.clear();
+      for (size_t q = 0; q < np; ++q) {
+        const uint32_t x = sr[sr.size() - 1 - 2 * q];
+        const uint32_t lanes = b.read_lengths[x] / stack_geom.rows + 1;
+        uint32_t it = kNoPair;
+        for (uint32_t f = lanes; f <= stack_geom.lanes && it == kNoPair; ++f)
+          if (!rc.bucket[f].empty()) {
+            it = rc.bucket[f].back();
+            rc.bucket[f].pop_back();
+          }
+        if (it == kNoPair) {
+          it = (uint32_t)rc.item_free.size();
+          rc.item_free.push_back(stack_geom.lanes);
+        }
+        rc.item_free[it] -= lanes;
+        rc.bucket[rc.item_free[it]].push_back(it);
+        rc.pair_item[q] = it;
+      }
+      // the items' pairs, item after item, each item's in placement order
+      const uint32_t nit = (uint32_t)rc.item_free.size();
+      rc.item_fill.assign(nit + 1, 0);
+      for (uint32_t it : rc.pair_item) rc.item_fill[it + 1] += 2;
+      for (uint32_t it = 0; it < nit; ++it) rc.item_fill[it + 1] += rc.item_fill[it];
+      rc.item_lens.resize(np);
+      rc.item_cls.resize(nit);
+      {
+        std::vector<uint32_t>& at = rc.item_free;  // reused: next pair slot per item
+        for (uint32_t it = 0; it < nit; ++it) at[it] = rc.item_fill[it] / 2;
+        for (size_t q = 0; q < np; ++q)
+          rc.item_lens[at[rc.pair_item[q]]++] = b.read_lengths[sr[sr.size() - 1 - 2 * q]];
+      }
+      for (uint32_t it = 0; it < nit; ++it) {
+        const uint32_t p0 = rc.item_fill[it] / 2, p1 = rc.item_fill[it + 1] / 2;
+        const ChainGeom& g = cheapest(rc.item_lens.data() + p0, p1 - p0);
+        rc.item_cls[it] = g.cls;
+        cost += g.cost;
+      }
+      if (nU & 1) cost += 0.5 * pair_cost(b.read_lengths[sr[m]]);
+      stacked = cost < classic;
+    }
+    if (!stacked) {
+      size_t i = m;
+      for (; i + 1 < sr.size(); i += 2) add_pair(sr[i], sr[i + 1]);
+      if (i < sr.size()) rc.leftover = sr[i];
+      return;
+    }
+    const uint32_t nit = (uint32_t)rc.item_cls.size();
+    const uint32_t base = (uint32_t)rc.reads.size();
+    rc.reads.resize(base + 2 * np);
+    for (uint32_t it = 0; it < nit; ++it)
+      rc.items.push_back(ChainPairs{rc.item_cls[it], base + rc.item_fill[it],
+                                    (rc.item_fill[it + 1] - rc.item_fill[it]) / 2});
+    for (size_t q = 0; q < np; ++q) {
+      uint32_t& at = rc.item_fill[rc.pair_item[q]];
+      rc.reads[base + at] = sr[sr.size() - 1 - 2 * q];
+      rc.reads[base + at + 1] = sr[sr.size() - 2 - 2 * q];
+      at += 2;
+    }
+    if (nU & 1) rc.leftover = sr[m];
+  };
   std::vector<uint32_t> rc((size_t)G * K, 0);      // reads of class c in region g
-  std::vector<uint32_t> rpairs((size_t)G * K, 0);  // read pairs (or single reads) of chain class c
+  std::vector<uint32_t> rpairs((size_t)G * K, 0);  // bin pairs of chain class c in region g
   std::vector<uint32_t> chains((size_t)G * K, 0);  // chain items of class c in region g
   std::vector<uint64_t> cpairs((size_t)G * K, 0);  // pairs those chains compute
+  std::vector<uint32_t> nstack((size_t)G * K, 0);  // reads in those bins (stack list entries)
   std::vector<uint64_t> hsum(G, 0);
   std::vector<uint32_t> hmax(G, 0);
   // multi-pass leftovers: the last read of each multi-pass class in the region
@@ -561,6 +722,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   std::vector<uint32_t> single_read(G, kNoPair);
   parallel_for(G, 16, [&](size_t lo, size_t hi) {
     std::vector<uint32_t> sr;
+    RegionChains chs;
     for (size_t g = lo; g < hi; ++g) {
       const rodv_region& rg = b.regions[g];
       for (uint32_t r = 0; r < rg.num_reads; ++r) {
@@ -577,14 +739,15 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       }
       if (fp64) continue;
       sorted_single(rg, sr);
-      for (size_t k = 0; k < sr.size(); k += 2) {
-        const bool two = k + 1 < sr.size();
-        const int c = two ? pair_class(sr[k], sr[k + 1]) : read_class[sr[k]];
-        cpairs[g * K + c] += (uint64_t)rg.num_haps * (two ? 2 : 1);
-        if (two)
-          rpairs[g * K + c] += 1;
-        else
-          single_read[g] = sr[k];
+      region_chains(sr, chs);
+      for (const ChainPairs& ci : chs.items) {
+        rpairs[g * K + ci.cls] += 1;
+        nstack[g * K + ci.cls] += 2 * ci.pairs;
+        cpairs[g * K + ci.cls] += (uint64_t)rg.num_haps * 2 * ci.pairs;
+      }
+      if (chs.leftover != kNoPair) {
+        single_read[g] = chs.leftover;
+        cpairs[g * K + read_class[chs.leftover]] += rg.num_haps;
       }
     }
   });
@@ -624,9 +787,10 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   std::stable_sort(order.begin(), order.end(),
                    [&](uint32_t x, uint32_t y) { return hsum[x] > hsum[y]; });
   // prefix offsets (within each class) of same/chain items, leftovers, FP64 list entries
-  std::vector<uint64_t> same_off((size_t)G * K), left_off((size_t)G * K), list_off((size_t)G * K);
+  std::vector<uint64_t> same_off((size_t)G * K), left_off((size_t)G * K), list_off((size_t)G * K),
+      stack_off((size_t)G * K);
   uint64_t same_tot[kNumClasses] = {}, left_tot[kNumClasses] = {}, list_tot[kNumClasses] = {},
-           cap_tot[kNumClasses] = {};
+           cap_tot[kNumClasses] = {}, stack_tot[kNumClasses] = {};
   for (uint32_t i = 0; i < G; ++i) {
     const uint32_t g = order[i];
     const uint64_t H = b.regions[g].num_haps;
@@ -635,6 +799,8 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       same_off[(size_t)g * K + c] = same_tot[c];
       left_off[(size_t)g * K + c] = left_tot[c];
       list_off[(size_t)g * K + c] = list_tot[c];
+      stack_off[(size_t)g * K + c] = stack_tot[c];
+      stack_tot[c] += nstack[(size_t)g * K + c];
       list_tot[c] += H * n;
       if (class_multi(c)) {
         same_tot[c] += H * (n / 2);
@@ -692,6 +858,8 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
     plan.off_same[c] = o;
     const size_t item = class_multi(c) ? sizeof(SameItem) : sizeof(ChainItem);
     o = align_up(o + (size_t)plan.same_items[c] * item);
+    plan.off_stack[c] = o;  // chain items' bins
+    if (!fp64 && !class_multi(c)) o = align_up(o + (size_t)stack_tot[c] * 4);
   }
   for (int c = 0; c < kNumClasses; ++c) {
     plan.off_diff[c] = o;
@@ -808,6 +976,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   parallel_for(G, 16, [&](size_t lo, size_t hi) {
     std::vector<uint32_t> byclass[kNumClasses];
     std::vector<uint32_t> sr;
+    RegionChains chs;
     for (size_t g = lo; g < hi; ++g) {
       const rodv_region& rg = b.regions[g];
       const uint32_t N = rg.num_reads;
@@ -817,15 +986,23 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       };
       if (!fp64) {
         sorted_single(rg, sr);
-        uint64_t next[kNumClasses];
-        for (int c = 0; c < kNumClasses; ++c) next[c] = same_off[g * K + c];
-        for (size_t k = 0; k + 1 < sr.size(); k += 2) {
-          const int c = pair_class(sr[k], sr[k + 1]);
+        region_chains(sr, chs);
+        uint64_t next[kNumClasses], snext[kNumClasses];
+        for (int c = 0; c < kNumClasses; ++c) {
+          next[c] = same_off[g * K + c];
+          snext[c] = stack_off[g * K + c];
+        }
+        for (const ChainPairs& cb : chs.items) {
+          const int c = cb.cls;
           ChainItem* ci = reinterpret_cast<ChainItem*>(s + plan.off_same[c]);
+          uint32_t* stk = reinterpret_cast<uint32_t*>(s + plan.off_stack[c]);
+          const uint32_t e0 = (uint32_t)snext[c];
+          for (uint32_t j = 0; j < 2 * cb.pairs; ++j) stk[snext[c]++] = chs.reads[cb.first + j];
           const uint32_t cap = plan.chain_haps[c];
           for (uint32_t h0 = 0; h0 < rg.num_haps; h0 += cap)
-            ci[next[c]++] = ChainItem{rg.hap_start + h0, std::min(cap, rg.num_haps - h0), sr[k],
-                                      sr[k + 1], out_of(h0, sr[k]), N, hmax[g], 0};
+            ci[next[c]++] = ChainItem{rg.hap_start + h0, std::min(cap, rg.num_haps - h0), e0,
+                                      cb.pairs, out_of(h0, rg.read_start), N, hmax[g],
+                                      rg.read_start};
         }
         if (single_read[g] != kNoPair) {
           const uint32_t rr = single_read[g];
@@ -935,6 +1112,7 @@ rodv_status Engine::launch_fp32_class(const PackedPlan& plan, uint8_t* dbase, in
   cl.scratch = class_scratch(plan, a, c);
   cl.scratch_cols = plan.scratch_cols;
   cl.error_flags = a.counts + kCtrError;
+  cl.stack = reinterpret_cast<const uint32_t*>(dbase + plan.off_stack[c]);
   if (class_multi(c)) {  // rescues at their items' positions: same items, then two-haplotype
     cl.flags |= kLaunchRescueByItem;
     cl.rescue_base = same ? 0u : 2u * plan.same_items[c];
@@ -1419,15 +1597,16 @@ rodv_status Engine::plain(rodv_device_batch* db, double* out, rodv_stats* st) {
   const PackedPlan& plan = db->plan;
   uint8_t* d = static_cast<uint8_t*>(db->arena.ptr);
   ArenaView a = arena_view(plan, d, tab_);
-  // control block: [0,24) ChainItem (one haplotype, one read) or SameItem
-  // (multi-pass), [32,44) rescue PairRef, words 12..15: fp32 counter, fp64
-  // counter, rescue count, error flags
+  // control block: [0,32) ChainItem (one haplotype, one read pair) or
+  // SameItem (multi-pass), [32,44) rescue PairRef, words 12..15: fp32
+  // counter, fp64 counter, rescue count, error flags, words 16..17: the
+  // chain item's pair (the read, kNoPair)
   DeviceMem ctl;
-  RODV_CUDA(ctl.ensure(64));
+  RODV_CUDA(ctl.ensure(72));
   uint8_t* w = static_cast<uint8_t*>(ctl.ptr);
   uint32_t* wc = reinterpret_cast<uint32_t*>(w + 48);
   PinnedMem host;
-  RODV_CUDA(host.ensure(64));
+  RODV_CUDA(host.ensure(72));
   uint8_t* hw = static_cast<uint8_t*>(host.ptr);
   uint32_t* hc = reinterpret_cast<uint32_t*>(hw + 48);
   uint32_t launches = 0;
@@ -1444,14 +1623,16 @@ rodv_status Engine::plain(rodv_device_batch* db, double* out, rodv_stats* st) {
           const SameItem item{rg.hap_start + h, read, kNoPair, (uint32_t)p};
           std::memcpy(hw, &item, sizeof(item));
         } else {
-          const ChainItem item{rg.hap_start + h, 1, read, kNoPair, (uint32_t)p, 0,
-                               plan.hap_len[rg.hap_start + h], 0};
+          const ChainItem item{rg.hap_start + h, 1, 0, 1, (uint32_t)p, 0,
+                               plan.hap_len[rg.hap_start + h], read};
           std::memcpy(hw, &item, sizeof(item));
         }
         const PairRef ref{rg.hap_start + h, read, (uint32_t)p};
         std::memcpy(hw + 32, &ref, sizeof(ref));
+        const uint32_t pair[2] = {read, kNoPair};
+        std::memcpy(hw + 64, pair, sizeof(pair));
         hc[0] = hc[1] = hc[2] = hc[3] = 0;
-        RODV_CUDA(cudaMemcpyAsync(w, hw, 64, cudaMemcpyHostToDevice, stream_));
+        RODV_CUDA(cudaMemcpyAsync(w, hw, 72, cudaMemcpyHostToDevice, stream_));
         for (int pass = 0; pass < 2; ++pass) {
           const bool f64 = pass == 1 || plan.fp64;
           const KernelInfo k =
@@ -1468,6 +1649,7 @@ rodv_status Engine::plain(rodv_device_batch* db, double* out, rodv_stats* st) {
           cl.scratch = class_scratch(plan, a, c);
           cl.scratch_cols = plan.scratch_cols;
           cl.error_flags = wc + 3;
+          cl.stack = reinterpret_cast<const uint32_t*>(w + 64);
           void* args[] = {&a.view, &cl};
           RODV_CUDA(
               cudaLaunchKernel(k.fn, dim3(1), dim3(k.threads), args, k.smem_bytes, stream_));
@@ -1664,7 +1846,8 @@ rodv_status Engine::autotune(const char* cache_path, int force, int32_t* variant
       const bool f64 = prec == 1;
       auto* db = new rodv_device_batch();
       PinnedMem staging;
-      rodv_status s = pack(b, db->plan, staging, f64);
+      // one read per bin: each class's batch stays in its class
+      rodv_status s = pack(b, db->plan, staging, f64, false, false);
       cudaError_t e = s == RODV_OK ? db->arena.ensure(db->plan.total_bytes) : cudaSuccess;
       if (s == RODV_OK && e == cudaSuccess)
         e = cudaMemcpyAsync(db->arena.ptr, staging.ptr, db->plan.upload_bytes,

@@ -89,6 +89,7 @@ struct PackedPlan {
   uint32_t list_cap[kNumClasses] = {};
   size_t off_hap_codes = 0, off_read_rows = 0, off_haps = 0, off_reads = 0;
   size_t off_same[kNumClasses] = {};
+  size_t off_stack[kNumClasses] = {};      // chain items' bins: read indices (uint32)
   size_t off_diff[kNumClasses] = {};
   size_t off_lists[kNumClasses] = {};      // FP64 work lists (rescued or forced)
   size_t off_preset = 0;                   // forced FP64: list lengths (uploaded)
@@ -162,8 +163,11 @@ class Engine {
   rodv_status cuda_fail(cudaError_t e, const char* where);
 
  private:
+  // stack_uniform: uniform-gap reads may stack into bins of the R = 8 class
+  // (off: one read per bin, every class keeps its own reads; the autotuner's
+  // per-class batches)
   rodv_status pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& staging, bool fp64,
-                   bool raw = false);
+                   bool raw = false, bool stack_uniform = true);
   // parts: 1 = counter reset and FP32 launches, 2 = FP64 launches.  ev: null,
   // or three events recorded before the FP32 launches, between the two parts
   // and after the FP64 launches.  fan_out: each class's launches go to its own

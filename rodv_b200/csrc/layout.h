@@ -17,8 +17,10 @@
 //                     16-byte boundary.
 //   haps       HapDesc[], reads ReadDesc[]
 //   items      the FP32 kernels' work, two reads per warp (the two float
-//              halves of every f32x2 instruction): ChainItem (two reads
-//              against all haplotypes of their region, single-pass reads),
+//              halves of every f32x2 instruction): ChainItem (read pairs
+//              stacked down the lanes against all haplotypes of their
+//              region, single-pass reads; their read lists follow the
+//              class's items),
 //              SameItem (two reads against one haplotype, multi-pass reads) or
 //              DiffItem (two PairRef, the multi-pass leftovers)
 //   lists      PairRef[] per work class: the FP64 kernels' work (pairs the
@@ -80,22 +82,29 @@ struct SameItem {
   uint32_t out_x;
 };
 
-// Two reads of one region against consecutive haplotypes of the region
-// (up to kChainHaps), swept in one pass over their concatenated columns.  The
-// result of (haplotype hap_start + i, read_x) goes to out_x + i * stride;
-// read_y's to that index + (read_y - read_x).  read_y may be kNoPair.
-// norm_len is the length of the region's longest haplotype: row 0 of the
-// sweep is scaled by 2^120/norm_len, which depends on the region only, so a
-// pair's result does not depend on how the region was cut into chains.
+// Reads of one region against consecutive haplotypes of the region (up to
+// kChainHaps), swept in one pass over their concatenated columns.  The item
+// holds `pairs` read pairs, entries [stack, stack + 2 * pairs) of the
+// class's stack list (x read, then y read or kNoPair), one pair per run of
+// lanes down the warp: a pair takes floor(len / R) + 1 lanes of R rows for
+// its longer read (its rows, then at least one pass-through row), x in the
+// low float half of the f32x2 lanes and y in the high one, and each pair's
+// first lane starts at the chain's first column.  The result of (haplotype
+// hap_start + i, read r) goes to out0 + i * stride + (r - read_base): reads
+// of a region are contiguous and results are hap-major.  norm_len is the
+// length of the region's longest haplotype: row 0 of the sweep is scaled by
+// 2^120/norm_len, which depends on the region only, so a pair's result does
+// not depend on how the region was cut into chains, nor on the lanes, item
+// or kernel its read was given.
 struct alignas(16) ChainItem {
   uint32_t hap_start;
   uint32_t num_haps;
-  uint32_t read_x;
-  uint32_t read_y;
-  uint32_t out_x;
+  uint32_t stack;     // first entry of the item's read pairs in the class's stack list
+  uint32_t pairs;     // read pairs stacked down the lanes
+  uint32_t out0;      // out index of (hap_start, read_base)
   uint32_t stride;    // the region's read count
   uint32_t norm_len;
-  uint32_t pad_;
+  uint32_t read_base; // the region's first read
 };
 
 // Two arbitrary pairs; x has the longer (or equal) haplotype; y.read may be
@@ -161,6 +170,7 @@ struct ClassLaunch {
   uint32_t flags;              // kLaunch* bits
   uint32_t wait_polls;         // pipelined sweeps: polls before a wait gives up (0: default)
   uint32_t rescue_base;        // kLaunchRescueByItem: list position of item 0's first pair
+  const uint32_t* stack;       // chain items: their read pairs (read indices)
 };
 
 // ClassLaunch::flags.  Testing hook: the producers of a pipelined sweep

@@ -230,12 +230,12 @@ struct SlotInfo {
 
 // Per-group shared memory of a chain sweep beyond the emission table: the
 // column of the separator after each haplotype (the last one is the virtual
-// separator just past the chain's end), and the last lane's running sum (I of
-// its last row, a pass-through row; x and y halves) at the end of each
-// haplotype.
+// separator just past the chain's end) and the region's read count (the
+// stride of a read's results).  After the groups' ChainMeta a chain warp
+// keeps 32 words: where each lane parks its pair's sums (run_chain).
 struct ChainMeta {
-  float2 acc[kChainHaps];  // column sums of the last lane's last row (I, x and y halves)
-  uint32_t sep[kChainHaps + 4];  // kChainHaps + 1 used; padded to 16 bytes
+  uint32_t sep[kChainHaps + 3];  // kChainHaps + 1 used
+  uint32_t stride;
 };
 
 // GROUP: lanes per wavefront.  32 (the whole warp) for every kernel but the
@@ -267,7 +267,7 @@ struct Forward {
   // (the next 32 columns of the previous pass's last row, see run_item).
   static constexpr int kRingCells = 2 * kWarp;
   static constexpr int kSmemPerWarp =
-      Shape::kBytesPerWarp + (kChain ? kGroups * (int)sizeof(ChainMeta) : 0) +
+      Shape::kBytesPerWarp + (kChain ? kGroups * (int)sizeof(ChainMeta) + kWarp * 4 : 0) +
       (MULTI ? kRingCells * 3 * (int)sizeof(V) : 0);
 
   // Shuffles within a lane group (the row above comes from the previous lane
@@ -312,8 +312,8 @@ struct Forward {
   }
 
   // Emission tables and priors of this lane (table slot `lane`) for read rows
-  // first_row + [0, R) of the two slots (reads of L[s] rows starting at row
-  // word row_off[s]).
+  // first_row[s] + [0, R) of the two slots s (reads of L[s] rows starting at
+  // row word row_off[s]).
   // Rows past a read's end are pass-through rows: emission 0, mi = ii = 1,
   // md = 0 (in the uniform form mi*gapm = gapm, since M~ = M/gapm).
   //
@@ -333,8 +333,8 @@ struct Forward {
   // overflow for likely pairs on short haplotypes.)
   __device__ __forceinline__ static void load_rows(const BatchView& b, const uint32_t (&L)[2],
                                                    const uint64_t (&row_off)[2],
-                                                   uint32_t first_row, int lane, uint4* table,
-                                                   Priors& p) {
+                                                   const uint32_t (&first_row)[2], int lane,
+                                                   uint4* table, Priors& p) {
     RowPriors<S> u[2];
     S cs[2] = {S(1), S(1)};  // emission scale of rows before the last (kScaled)
     if (UNIFORM) {  // uniform-gap priors come from the read's first row
@@ -353,10 +353,10 @@ struct Forward {
     S* tab = reinterpret_cast<S*>(table);
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-      const uint32_t row = first_row + k;  // 0-based read row
       S mmv[2], gv[2], miv[2], iiv[2], mdv[2];
 #pragma unroll
       for (int s = 0; s < P::kSlots; ++s) {
+        const uint32_t row = first_row[s] + k;  // 0-based read row
         const bool real = row < L[s];
         const uint32_t w = real ? b.read_rows[row_off[s] + row] : 0u;
         const RowPriors<S> rp = row_priors<S>(w, b.tab);
@@ -395,10 +395,12 @@ struct Forward {
       }
     }
     if (kScaled) {
-      const uint32_t row = first_row + R;
       S iin[2];
 #pragma unroll
-      for (int s = 0; s < 2; ++s) iin[s] = row < L[s] ? u[s].ii : (row == L[s] ? u[s].mi : S(1));
+      for (int s = 0; s < 2; ++s) {
+        const uint32_t row = first_row[s] + R;
+        iin[s] = row < L[s] ? u[s].ii : (row == L[s] ? u[s].mi : S(1));
+      }
       p.iiN = P::make(iin[0], iin[1]);
     }
   }
@@ -682,7 +684,8 @@ struct Forward {
     for (uint32_t pass = 0; pass < passes; ++pass) {
       const bool last = (pass + 1 == passes);
       Priors pr;
-      load_rows(b, L, row_off, pass * (kWarp * R) + lane * R, lane, table, pr);
+      const uint32_t fr = pass * (kWarp * R) + lane * R;
+      load_rows(b, L, row_off, {fr, fr}, lane, table, pr);
 
       V M[R], I[R], D[R];
 #pragma unroll
@@ -797,22 +800,32 @@ struct Forward {
   // reference's); the DP is linear in it, so haplotype i's result is
   // rescaled by (2^120/H_i)/(2^120/norm_len) in FP64 before the acceptance
   // test and log10.
-  // `items`: the chain items of this warp, one per lane group; `count`: how
-  // many of them exist (a group without one repeats the first and writes
-  // nothing).
+  // `first`: the first chain item of this warp's lane groups (group g takes
+  // item first + g); `count`: how many items exist (a group without one
+  // repeats the first and writes nothing).
+  //
+  // Read pairs: lane e of a group fetches pair e, a scan of the pairs' lane
+  // counts gives each pair's first lane, and every lane then takes the pair
+  // covering it (lanes past the last pair extend its pass-through rows).  A
+  // lane's lag, its distance from its pair's first lane, is the step at which
+  // it reaches the chain's first column: a pair's first lane takes row 0's
+  // boundary from step 0, as lane 0 of a one-pair item does, and its last
+  // lane, whose last row is a pass-through row, parks the pair's sums.
   __device__ static void run_chain(const BatchView& b, const ClassLaunch& c, uint32_t first,
                                    uint32_t count, int lane, uint4* table) {
     const int grp = lane / GROUP;            // lane group
     const int gl = lane & (GROUP - 1);       // lane within its group
     const bool active = first + (uint32_t)grp < count;
-    ChainMeta* meta =
-        reinterpret_cast<ChainMeta*>(table + Shape::kBytesPerWarp / 16) + grp;
-    const ChainItem it =
-        static_cast<const ChainItem*>(c.work)[first + (active ? (uint32_t)grp : 0u)];
-    const bool has_y = it.read_y != kNoPair;
+    ChainMeta* const metas = reinterpret_cast<ChainMeta*>(table + Shape::kBytesPerWarp / 16);
+    ChainMeta* meta = metas + grp;
+    // per lane of the warp: the out index of (the item's first haplotype,
+    // the x read) where the lane parks its pair's sums, else kNoStore
+    uint32_t* park = reinterpret_cast<uint32_t*>(metas + kGroups);
+    constexpr uint32_t kNoStore = 0xffffffffu;
+    const ChainItem* item_ptr =
+        static_cast<const ChainItem*>(c.work) + first + (active ? (uint32_t)grp : 0u);
+    const ChainItem it = *item_ptr;
     const uint32_t n = it.num_haps;
-    const ReadDesc rx = b.reads[it.read_x];
-    const ReadDesc ry = b.reads[has_y ? it.read_y : it.read_x];
     // lane gl of a group holds haplotype gl's length and code offset
     uint32_t hl = 0;
     uint64_t co = 0;
@@ -822,15 +835,50 @@ struct Forward {
       co = hd.code_off;
     }
     const uint64_t co_next = __shfl_down_sync(kFullMask, co, 1, GROUP);
-    const bool bad_hap = (uint32_t)gl < n && (hl == 0 || ((uint32_t)gl + 1 < n &&
-                                                          co_next != co + hl + 1));
-    const uint32_t Lmax = rx.len > ry.len ? rx.len : ry.len;
-    const bool bad = bad_hap || hl > it.norm_len || n == 0 || n > (uint32_t)kGroupHaps ||
-                     rx.len == 0 || ry.len == 0 || Lmax >= (uint32_t)(GROUP * R);
+    const bool bad_counts = n == 0 || n > (uint32_t)kGroupHaps || it.pairs == 0 ||
+                            it.pairs > (uint32_t)GROUP;
+    bool bad = bad_counts || ((uint32_t)gl < n && (hl == 0 || hl > it.norm_len ||
+                                                   ((uint32_t)gl + 1 < n && co_next != co + hl + 1)));
+    // pair e at lane e: its reads and lanes
+    const bool holder = !bad_counts && (uint32_t)gl < it.pairs;
+    const uint32_t hrx = holder ? c.stack[it.stack + 2u * gl] : 0u;
+    const uint32_t hry = holder ? c.stack[it.stack + 2u * gl + 1u] : kNoPair;
+    const uint32_t lx = holder ? b.reads[hrx].len : 0u;
+    const uint32_t ly = (holder && hry != kNoPair) ? b.reads[hry].len : 0u;
+    bad = bad || (holder && (lx == 0 || (hry != kNoPair && ly == 0)));
+    const uint32_t hlanes = holder ? max(lx, ly) / R + 1 : 0u;
+    uint32_t end = hlanes;  // lanes of pairs 0..gl
+#pragma unroll
+    for (int d = 1; d < GROUP; d *= 2) {
+      const uint32_t v = __shfl_up_sync(kFullMask, end, d, GROUP);
+      if (gl >= d) end += v;
+    }
+    const uint32_t hstart = end - hlanes;
+    bad = bad || __shfl_sync(kFullMask, end, GROUP - 1, GROUP) > (uint32_t)GROUP;
     if (__any_sync(kFullMask, bad)) {
       if (lane == 0) atomicOr(c.error_flags, kErrChain);
       return;
     }
+    // the pair covering this lane
+    const uint32_t starts =
+        __reduce_or_sync(kFullMask, holder ? 1u << (hstart + (uint32_t)(grp * GROUP)) : 0u) >>
+        (grp * GROUP);
+    const int e = __popc(starts & ((2u << gl) - 1u)) - 1;
+    const uint32_t rx = __shfl_sync(kFullMask, hrx, e, GROUP);
+    const uint32_t ry0 = __shfl_sync(kFullMask, hry, e, GROUP);
+    const uint32_t st = __shfl_sync(kFullMask, hstart, e, GROUP);
+    const uint32_t nl = __shfl_sync(kFullMask, hlanes, e, GROUP);
+    const int lag = gl - (int)st;
+    // steps past the longer chain's last column for every pair's last lane
+    // to reach its virtual end separator
+    const uint32_t maxnl = __reduce_max_sync(kFullMask, hlanes);
+    const uint32_t ry = ry0 != kNoPair ? ry0 : rx;  // no y read: x again, not stored
+    const bool parks = active && (uint32_t)lag == nl - 1;
+    park[lane] = parks ? it.out0 + (rx - it.read_base) : kNoStore;
+    if (gl == 0) meta->stride = it.stride;
+    const ReadDesc dx = b.reads[rx], dy = b.reads[ry];
+    const uint32_t L[2] = {dx.len, dy.len};
+    const uint64_t row_off[2] = {dx.row_off, dy.row_off};
     // end column (exclusive) + 1 of haplotype gl in the chain's columns
     uint32_t endc = (uint32_t)gl < n ? hl + 1 : 0;
 #pragma unroll
@@ -848,34 +896,36 @@ struct Forward {
     const uint64_t co0 = __shfl_sync(kFullMask, co, 0, GROUP);
     const S init_s = P::init_const() / (S)it.norm_len;
     const V init = P::make(init_s, init_s);
-    const uint32_t L[2] = {rx.len, ry.len};
-    const uint64_t row_off[2] = {rx.row_off, ry.row_off};
     Priors pr;
-    load_rows(b, L, row_off, (uint32_t)(gl * R), lane, table, pr);
+    const uint32_t fr = (uint32_t)lag * R;  // this lane's first row in its pair's reads
+    load_rows(b, L, row_off, {fr, fr}, lane, table, pr);
     __syncwarp();
 
+    const bool top = lag == 0;  // a pair's first lane
     V M[R], I[R], D[R];
 #pragma unroll
     for (int k = 0; k < R; ++k) M[k] = I[k] = D[k] = P::zero();
     V dg_m = P::zero(), dg_i = P::zero(), dg_d = P::zero();
-    if (gl == 0) dg_d = init;
+    if (top) dg_d = init;
     // scaled form: the first row's M term of the previous column (row 0 of
-    // the DP, D^ = init, for the group's first lane)
-    V dg_t = gl == 0 ? init : P::zero();
-    const uint8_t* hx = b.hap_codes + co0 - gl;
+    // the DP, D^ = init, for a pair's first lane)
+    V dg_t = top ? init : P::zero();
+    // column s - lag at step s
+    const uint8_t* hx = b.hap_codes + co0 - lag;
     uint32_t hi = 0;                          // this lane's haplotype in the chain
-    int nxt = (int)meta->sep[0] + gl;         // step at which this lane is at the next separator
-    // Reads of a single-pass class are shorter than the rows the sweep holds
-    // (class_of), so the last lane's last row is a pass-through row: its M is
-    // 0 and its I carries the read's last-row value; one running sum
-    // (of I) gives the result.
+    int nxt = (int)meta->sep[0] + lag;        // step at which this lane is at the next separator
+    // Reads of a chain are shorter than the rows their lanes hold, so the
+    // last lane's last row of a pair is a pass-through row: its M is 0 and
+    // its I carries the read's last-row value; one running sum (of I) gives
+    // the result.
     V acc_i = P::zero();
-    // through the virtual end separator of the longer chain, for the last lane
-    const int nsteps = (int)span + GROUP;
+    // through the virtual end separator of the longer chain, for every
+    // pair's last lane
+    const int nsteps = (int)span + (int)maxnl;
     // A lane of the shorter chain of a two-group warp keeps stepping past its
     // virtual end separator (column ncols) with nothing left to compute; its
     // code index stays clamped there so it reads no byte past its chain.
-    const int last_s = (int)ncols + gl;
+    const int last_s = (int)ncols + lag;
 
     // the haplotype code of the next step is loaded one step ahead (the
     // emission loads wait on it); the sweep runs in blocks of kStepBlock
@@ -893,7 +943,7 @@ struct Forward {
         // the I^ of this lane's first row
         V in_t = group_shfl_up(P::fma(pr.mmU, M[R - 1], P::add(I[R - 1], D[R - 1])));
         V in_i = group_shfl_up(P::fma(pr.iiN, I[R - 1], M[R - 1]));
-        if (gl == 0) {
+        if (top) {
           in_t = init; in_i = P::zero();
         }
         load_emission(table, lane, code, 0u, e);
@@ -903,7 +953,7 @@ struct Forward {
         V up_m = group_shfl_up(M[R - 1]);
         V up_i = group_shfl_up(I[R - 1]);
         V up_d = group_shfl_up(D[R - 1]);
-        if (gl == 0) {
+        if (top) {
           up_m = P::zero(); up_i = P::zero(); up_d = init;
         }
         load_emission(table, lane, code, 0u, e);
@@ -914,12 +964,15 @@ struct Forward {
       if (s == nxt) {  // this lane just computed a separator column
 #pragma unroll
         for (int k = 0; k < R; ++k) D[k] = P::zero();
-        if (gl == GROUP - 1) {
-          meta->acc[hi] = make_float2(P::sx(acc_i), P::sy(acc_i));
-          acc_i = P::zero();
-        }
+        // a pair's sums over haplotype hi (x and y halves), parked in the x
+        // read's result slot until the sweep ends
+        const uint32_t px = park[lane];
+        if (px != kNoStore)
+          reinterpret_cast<float2*>(b.out)[px + hi * meta->stride] =
+              make_float2(P::sx(acc_i), P::sy(acc_i));
+        acc_i = P::zero();
         ++hi;
-        nxt = (int)meta->sep[hi] + gl;
+        nxt = (int)meta->sep[hi] + lag;
       }
     };
     // Blocks of kStepBlock fully unrolled steps: the compiler overlaps
@@ -934,25 +987,34 @@ struct Forward {
 #pragma unroll
       for (int i = 0; i < kStepBlock; ++i) step(s0 + i);
     }
+    // the parked sums (written by other lanes of the warp) to results; the
+    // item is read again rather than kept in registers through the sweep
     __syncwarp();
-    if (active && (uint32_t)gl < n) {
-      const float2 a = meta->acc[gl];
-      const double ratio = (double)(P::init_const() / (S)hl) / (double)init_s;
-      const uint32_t hap = it.hap_start + gl;
-      const uint32_t out = it.out_x + (uint32_t)gl * it.stride;
-      double res_x, res_y = 0.0;
-      double amin_x = (double)kMinAcceptedF, amin_y = (double)kMinAcceptedF;
-      if (kScaled) {  // the pass-through row holds (M_L + I_L)/gapm: the sum / mi
-        res_x = scaled_result(b, it.read_x, rx.len, GROUP * R, 0.f, a.x, &amin_x);
-        if (has_y) res_y = scaled_result(b, it.read_y, ry.len, GROUP * R, 0.f, a.y, &amin_y);
-      } else {        // the pass-through row holds M_L + I_L (its M is 0)
-        res_x = a.x;
-        res_y = a.y;
+    if (active) {
+      const ChainItem ci = *item_ptr;
+      const uint32_t nh = ci.num_haps;
+      const uint32_t ne = ci.pairs * nh;
+      for (uint32_t p = (uint32_t)gl; p < ne; p += GROUP) {
+        const uint32_t q = p / nh, h = p - q * nh;  // pair q of the item, haplotype h
+        const uint32_t base = ci.out0 + h * ci.stride - ci.read_base;
+        const uint32_t read[2] = {c.stack[ci.stack + 2 * q], c.stack[ci.stack + 2 * q + 1]};
+        const float2 a = reinterpret_cast<const float2*>(b.out)[base + read[0]];
+        const double ratio =
+            (double)(P::init_const() / (S)b.haps[ci.hap_start + h].len) / (double)init_s;
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+          if (read[s] == kNoPair) continue;
+          const S sum = s == 0 ? a.x : a.y;
+          double res, amin = (double)kMinAcceptedF;
+          if (kScaled) {  // the pass-through row holds (M_L + I_L)/gapm: the sum / mi
+            const uint32_t len = b.reads[read[s]].len;
+            res = scaled_result(b, read[s], len, len + 1, S(0), sum, &amin);
+          } else {        // the pass-through row holds M_L + I_L (its M is 0)
+            res = sum;
+          }
+          finish(b, c, PairRef{ci.hap_start + h, read[s], base + read[s]}, res * ratio, amin);
+        }
       }
-      finish(b, c, PairRef{hap, it.read_x, out}, res_x * ratio, amin_x);
-      if (has_y)
-        finish(b, c, PairRef{hap, it.read_y, out + (it.read_y - it.read_x)}, res_y * ratio,
-               amin_y);
     }
     __syncwarp();
   }

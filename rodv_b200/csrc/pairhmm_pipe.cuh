@@ -275,7 +275,8 @@ struct PipeForward {
       };
 
       typename F::Priors pr;
-      F::load_rows(b, L, row_off, p * (kWarp * R) + lane * R, lane, table, pr);
+      const uint32_t fr = p * (kWarp * R) + lane * R;
+      F::load_rows(b, L, row_off, {fr, fr}, lane, table, pr);
       V M[R], I[R], D[R];
 #pragma unroll
       for (int k = 0; k < R; ++k) M[k] = I[k] = D[k] = P::zero();
