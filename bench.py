@@ -20,8 +20,8 @@ Reported (see the JSON keys):
              this GPU in this run (FMA-chain kernels, rodv_measure_peaks);
              12 algorithmic flops per cell (4 mul + 2 add for M, 2 mul + 1 add
              for I and for D); traffic is the DRAM bytes of those kernels per
-             step, from an ncu capture of the dominant class's kernel on the
-             same sources (profiles/), scaled to the step by its cell share.
+             step, from an ncu capture of every FP32 launch of one step at a
+             smaller scale on the same sources (profiles/), scaled by cells.
   plain_form the plain GPU form (one launch per pair) against the batched
              engine on the same sample.
   cpu_baseline  the reference's own schedule_pairhmm (oracle/_ref), threads
@@ -56,7 +56,7 @@ FLOPS_PER_CELL = 12
 # every result must be within this many log10 units of the FP64 oracle and of
 # the reference's own output
 ACCURACY_TOL = 1e-3
-TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "forward_kernel_dram_traffic_uneven.md")
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "forward_kernels_dram_traffic_uneven.md")
 # The device sources whose compiled code the traffic capture measured.
 KERNEL_SOURCES = ["pairhmm_fwd.cuh", "pairhmm_pipe.cuh", "layout.h", "kernel_table.cuh",
                   "kernels.h", "pairhmm_kernels.cu", "kernels_r*.cu", "kernels_multi_r*.cu"]
@@ -116,10 +116,10 @@ def profile_fields(path=TRAFFIC_PROFILE):
 
 def step_traffic_bytes(workload, scale):
     """DRAM bytes (read + write) of the FP32 kernels of one resident step of the
-    full-size uneven workload: the capture of the dominant class's kernel in
-    TRAFFIC_PROFILE, scaled to the step by that class's share of the step's
-    cells.  Returns (bytes or None, note).  A capture taken on other kernel
-    sources than these is not reported (the note says so)."""
+    full-size uneven workload: the capture of every FP32 launch of one step of
+    the same workload at a smaller scale in TRAFFIC_PROFILE, scaled by the
+    step's cells.  Returns (bytes or None, note).  A capture taken on other
+    kernel sources than these is not reported (the note says so)."""
     if workload != "uneven" or scale != 1.0:
         return None, "captured for the full-size uneven workload only"
     f = profile_fields()
@@ -129,42 +129,6 @@ def step_traffic_bytes(workload, scale):
         return None, ("STALE: the traffic capture measured kernel sources "
                       f"{f.get('kernel_source_sha16')}, this build has {kernel_source_sha()}")
     return int(f["fp32_step_traffic_bytes"]), f.get("traffic_note", "")
-
-
-def chain_class_cells(batch):
-    """Cells each single-pass chain class computes in the FP32 pass, keyed by
-    (rows per lane, uniform gaps): the packer's pairing restated (engine.cu,
-    pack): a region's single-pass reads sorted by (uniform gaps, length) pair
-    up neighbour by neighbour, and a pair's chain items are of the class of
-    its longer read (uniform only if both are); an odd last read goes to the
-    two-haplotype kernel instead.  Scales a one-class traffic capture to a
-    step."""
-    rl = batch.read_lengths.astype(np.int64)
-    hl = batch.hap_lengths.astype(np.int64)
-    ro = batch.read_offsets.astype(np.int64)
-    const = np.ones(len(rl), dtype=bool)
-    first = {}
-    for name in ("ins_quals", "del_quals", "gcp_quals"):
-        q = getattr(batch, name).astype(np.int64) & 127
-        first[name] = q[ro]
-        if len(q):
-            const &= (np.maximum.reduceat(q, ro) == np.minimum.reduceat(q, ro))
-    ins, gcp = first["ins_quals"], first["gcp_quals"]
-    uni = (const & (ins == first["del_quals"]) & (gcp != 0) &
-           (10.0 ** (-ins / 10.0) * (1.0 - 10.0 ** (-gcp / 10.0)) >= 1e-6))
-    key = (uni.astype(np.int64) << 20) | rl
-    out = {}
-    for rg in batch.regions:
-        h0, r0 = int(rg["hap_start"]), int(rg["read_start"])
-        hsum = int(hl[h0:h0 + int(rg["num_haps"])].sum())
-        reads = np.arange(r0, r0 + int(rg["num_reads"]))
-        single = reads[rl[reads] < 256]
-        s = single[np.argsort(key[single], kind="stable")]
-        for k in range(0, len(s) - 1, 2):
-            x, y = s[k], s[k + 1]
-            c = (int(max(rl[x], rl[y])) // 32 + 1, bool(uni[x] and uni[y]))
-            out[c] = out.get(c, 0) + hsum * int(rl[x] + rl[y])
-    return out
 
 
 def log(*a):
@@ -446,8 +410,8 @@ def run_engine(args, world, rank, local):
                          "unit": "TFLOP/s", "frac": achieved / peak,
                          "traffic": traffic,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
-                                           "of the dominant FP32 class kernel, scaled to one "
-                                           "step by its cell share (" +
+                                           "of every FP32 launch of one step at a smaller "
+                                           "scale, scaled to this step by its cells (" +
                                            os.path.relpath(TRAFFIC_PROFILE, ROOT) + "); " +
                                            traffic_note,
                          "kernel_source_sha16": kernel_source_sha(),

@@ -55,7 +55,7 @@ def test_roofline_traffic_comes_from_a_capture_of_these_kernels():
     import bench
     f = bench.profile_fields()
     assert f.get("kernel_source_sha16") == bench.kernel_source_sha(), (
-        "profiles/forward_kernel_dram_traffic_uneven.md was captured on other kernel "
+        "profiles/forward_kernels_dram_traffic_uneven.md was captured on other kernel "
         "sources; capture it again")
     t, note = bench.step_traffic_bytes("uneven", 1.0)
     assert t is not None and 2e8 < t < 5e9, note
