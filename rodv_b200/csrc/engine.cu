@@ -313,10 +313,7 @@ rodv_status Engine::init() {
   tab_.mm_d = static_cast<const double*>(put(t.mm_d.data(), kMmTableSize * 8));
   RODV_CUDA(ce);
   // Kernels whose tables exceed the default 48 KB of dynamic shared memory
-  // per block opt in to their size.  The chain kernels also prefer the
-  // largest shared-memory carveout: with the driver's default split an SM
-  // held 4 blocks of the R = 8 kernel (42 KB each) where 228 KB hold 5, so
-  // the occupancy targets above 4 blocks/SM were not reached.
+  // per block opt in to their size.
   for (int c = 0; c < kNumClasses; ++c)
     for (int p = 0; p < 3; ++p)
       for (int v = 0; v < kTuneVariants; ++v) {
@@ -327,9 +324,6 @@ rodv_status Engine::init() {
         if (k.fn && k.smem_bytes > 48 * 1024)
           RODV_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          k.smem_bytes));
-        if (k.fn && k.chain)
-          RODV_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                         (int)cudaSharedmemCarveoutMaxShared));
       }
   ready_ = true;
   if (opt_.tune_cache && opt_.tune_cache[0]) load_tuning(opt_.tune_cache);
