@@ -274,7 +274,7 @@ rodv_status rodv_pairhmm_batch_noalloc(const rodv_batch* batch, int32_t use_doub
  * every variant of the class's kernels on a synthetic batch of that class
  * and keeps the fastest.  Single-pass classes: the FP32 kernel's occupancy
  * target (register budget) and, for reads up to 128 bases, one or two chain
- * items per warp.  Multi-pass classes (reads over 256 bases): the strip
+ * items per warp.  Multi-pass classes (reads of 255 bases and more): the strip
  * height (4 or 8 read rows per lane per pass) and the warps that sweep one
  * item's passes concurrently (2 or 4), for the FP32 and the FP64 kernel.
  * Results do not depend on the variants.  No counterpart in the reference,

@@ -588,20 +588,23 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   };
   ChainGeom geom[kMaxRowsPerLane + 1] = {};
   for (int R = 1; R <= kMaxRowsPerLane; ++R) {
-    const int c = class_of((uint32_t)(R * kWarp) - 1, true);
+    const int c = single_pass_class(R, true);
     const int ipw = forward_kernel_info(Precision::kF32x2, R, true, false, true, variant_[c])
                         .items_per_warp;
     geom[R] = ChainGeom{c, (uint32_t)(kWarp / ipw), (uint32_t)(R * ipw),
                         R * kChainCellCost[R]};
   }
   const ChainGeom& stack_geom = geom[kMaxRowsPerLane];
+  // lanes of `rows` rows a uniform-gap read pair takes whose longer read has
+  // len bases: its rows, a pass-through row and the row that sums it
+  auto pair_lanes = [](uint32_t len, uint32_t rows) { return (len + 1) / rows + 1; };
   // the cheapest uniform class whose items hold pairs with longer reads of
   // lengths lens
   auto cheapest = [&](const uint32_t* lens, size_t n) -> const ChainGeom& {
     const ChainGeom* best = &stack_geom;
     for (int R = 1; R < kMaxRowsPerLane; ++R) {
       uint32_t lanes = 0;
-      for (size_t i = 0; i < n; ++i) lanes += lens[i] / geom[R].rows + 1;
+      for (size_t i = 0; i < n; ++i) lanes += pair_lanes(lens[i], geom[R].rows);
       if (lanes <= geom[R].lanes && geom[R].cost < best->cost) best = &geom[R];
     }
     return *best;
@@ -635,7 +638,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
     // Stacked: neighbours in decreasing length pair up (the shortest read
     // of an odd count is the leftover), the pairs go by best fit in that
     // order into items of the R = 8 class (a pair takes the item with the
-    // fewest free lanes that still holds its len/8 + 1 lanes), and each item
+    // fewest free lanes that still holds its (len+1)/8 + 1 lanes), and each item
     // then goes to the cheapest uniform class that holds its pairs.
     const size_t np = nU / 2;
     bool stacked = false;
@@ -646,7 +649,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       for (auto& v : rc.bucket) v.clear();
       for (size_t q = 0; q < np; ++q) {
         const uint32_t x = sr[sr.size() - 1 - 2 * q];
-        const uint32_t lanes = b.read_lengths[x] / stack_geom.rows + 1;
+        const uint32_t lanes = pair_lanes(b.read_lengths[x], stack_geom.rows);
         uint32_t it = kNoPair;
         for (uint32_t f = lanes; f <= stack_geom.lanes && it == kNoPair; ++f)
           if (!rc.bucket[f].empty()) {
@@ -714,6 +717,7 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
   std::vector<uint32_t> left_read((size_t)G * 2, kNoPair);
   // single-pass leftover: the odd last read of the region's sorted single-pass reads
   std::vector<uint32_t> single_read(G, kNoPair);
+  std::atomic<bool> chain_class_bad{false};  // a chain item outside the single-pass classes
   parallel_for(G, 16, [&](size_t lo, size_t hi) {
     std::vector<uint32_t> sr;
     RegionChains chs;
@@ -735,6 +739,10 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       sorted_single(rg, sr);
       region_chains(sr, chs);
       for (const ChainPairs& ci : chs.items) {
+        if (ci.cls < 0 || ci.cls >= kSinglePassClasses) {
+          chain_class_bad.store(true);
+          break;
+        }
         rpairs[g * K + ci.cls] += 1;
         nstack[g * K + ci.cls] += 2 * ci.pairs;
         cpairs[g * K + ci.cls] += (uint64_t)rg.num_haps * 2 * ci.pairs;
@@ -745,6 +753,8 @@ rodv_status Engine::pack(const rodv_batch& b, PackedPlan& plan, PinnedMem& stagi
       }
     }
   });
+  if (chain_class_bad.load())
+    return fail(RODV_ERR_INTERNAL, "packer placed a chain item outside the single-pass classes");
   // Haplotypes per chain item, per class: the longest chains (up to
   // kChainHaps) that still leave every resident warp of the class's launch
   // (16 per SM at most) two items; a small batch gets short chains (down to

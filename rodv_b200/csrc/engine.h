@@ -20,14 +20,18 @@ namespace rodv {
 constexpr int kSinglePassClasses = kMaxRowsPerLane * 2;
 constexpr int kNumClasses = kSinglePassClasses + 2;
 
-// A single-pass class holds reads of up to 32R - 1 bases (R = floor(L/32) + 1):
-// the sweep's last row is always a pass-through row, so one running sum
-// gives the result.  Reads of 256 bases and more are multi-pass.
+// A single-pass sweep holds a read's rows, then at least one pass-through
+// row (so one running sum gives the result) and, in the uniform-gap (scaled)
+// form, the row whose D sums that pass-through row over each haplotype's
+// columns: a class of R rows per lane holds reads of up to 32R - 1 bases
+// with per-row gaps and 32R - 2 with uniform gaps.  Longer reads are
+// multi-pass.
+// The single-pass class of R rows per lane and the given gap form.
+inline int single_pass_class(int R, bool uniform) { return (R - 1) * 2 + (uniform ? 1 : 0); }
 inline int class_of(uint32_t read_len, bool uniform) {
-  if (read_len < (uint32_t)kPassRows) {
-    const int R = (int)(read_len / kWarp) + 1;
-    return (R - 1) * 2 + (uniform ? 1 : 0);
-  }
+  const uint32_t rows = read_len + (uniform ? 2u : 1u);
+  if (rows <= (uint32_t)kPassRows)
+    return single_pass_class((int)((rows + kWarp - 1) / kWarp), uniform);
   return kSinglePassClasses + (uniform ? 1 : 0);
 }
 inline int class_rows(int cls) { return cls < kSinglePassClasses ? cls / 2 + 1 : kMaxRowsPerLane; }

@@ -331,10 +331,13 @@ struct Forward {
   // pass-through row, and sum(M~_L)/mi + sum(I^_L) when it is row L itself.
   // (Scaling row L by 1/mi instead would make the next row's (mm/c)*M~
   // overflow for likely pairs on short haplotypes.)
+  // sum_lane (scaled form, chain sweeps): this lane's last row is a pair's
+  // sum row, a pass-through row with emission 1 for every code (run_chain).
   __device__ __forceinline__ static void load_rows(const BatchView& b, const uint32_t (&L)[2],
                                                    const uint64_t (&row_off)[2],
                                                    const uint32_t (&first_row)[2], int lane,
-                                                   uint4* table, Priors& p) {
+                                                   uint4* table, Priors& p,
+                                                   bool sum_lane = false) {
     RowPriors<S> u[2];
     S cs[2] = {S(1), S(1)};  // emission scale of rows before the last (kScaled)
     if (UNIFORM) {  // uniform-gap priors come from the read's first row
@@ -393,6 +396,12 @@ struct Forward {
         p.gapm[UNIFORM ? 0 : k] = P::make(gv[0], gv[1]);
         p.md[UNIFORM ? 0 : k] = P::make(mdv[0], mdv[1]);
       }
+    }
+    if (kScaled && sum_lane) {
+#pragma unroll
+      for (int s = 0; s < P::kSlots; ++s)
+#pragma unroll
+        for (int code = 0; code < kNumCodes; ++code) put_emission(tab, s, code, R - 1, lane, S(1));
     }
     if (kScaled) {
       S iin[2];
@@ -491,7 +500,11 @@ struct Forward {
   // (mm/c)*M~_d + I^_d + D^_d and i0 its I^, both computed by the lane above
   // with the same operations cells() would apply here, so the results are
   // bitwise the same while the lanes exchange two values a step instead of
-  // three.
+  // three.  D takes each row's ii: the read's dd on its rows (uniform gaps:
+  // ii == dd, the value cells() uses), and 1 on pass-through rows below row
+  // L, where M is 0 and D stays 0 -- except on a chain sweep's sum row, whose
+  // emission 1 makes its M the pass-through value one column back and its D
+  // the exact running sum of the earlier ones (run_chain).
   __device__ __forceinline__ static void cells_scaled(const V (&e)[R], V t0, V i0, V (&M)[R],
                                                       V (&I)[R], V (&D)[R], const Priors& p,
                                                       V& t_last) {
@@ -503,7 +516,7 @@ struct Forward {
       M[k] = P::mul(t, e[k]);
       if (k == R - 1) t_last = t;
       I[k] = k == 0 ? i0 : P::fma(p.ii[k], ui, um);
-      D[k] = P::fma(p.ddU, oD, oM);
+      D[k] = P::fma(p.ii[k], oD, oM);
       dm = oM; di = oI; dd = oD;
       um = M[k]; ui = I[k];
     }
@@ -846,7 +859,9 @@ struct Forward {
     const uint32_t lx = holder ? b.reads[hrx].len : 0u;
     const uint32_t ly = (holder && hry != kNoPair) ? b.reads[hry].len : 0u;
     bad = bad || (holder && (lx == 0 || (hry != kNoPair && ly == 0)));
-    const uint32_t hlanes = holder ? max(lx, ly) / R + 1 : 0u;
+    // rows of a pair: its longer read's, a pass-through row and, in the
+    // scaled form, the sum row
+    const uint32_t hlanes = holder ? (max(lx, ly) + (kScaled ? 1u : 0u)) / R + 1 : 0u;
     uint32_t end = hlanes;  // lanes of pairs 0..gl
 #pragma unroll
     for (int d = 1; d < GROUP; d *= 2) {
@@ -898,7 +913,7 @@ struct Forward {
     const V init = P::make(init_s, init_s);
     Priors pr;
     const uint32_t fr = (uint32_t)lag * R;  // this lane's first row in its pair's reads
-    load_rows(b, L, row_off, {fr, fr}, lane, table, pr);
+    load_rows(b, L, row_off, {fr, fr}, lane, table, pr, (uint32_t)lag == nl - 1);
     __syncwarp();
 
     const bool top = lag == 0;  // a pair's first lane
@@ -914,10 +929,14 @@ struct Forward {
     const uint8_t* hx = b.hap_codes + co0 - lag;
     uint32_t hi = 0;                          // this lane's haplotype in the chain
     int nxt = (int)meta->sep[0] + lag;        // step at which this lane is at the next separator
-    // Reads of a chain are shorter than the rows their lanes hold, so the
-    // last lane's last row of a pair is a pass-through row: its M is 0 and
-    // its I carries the read's last-row value; one running sum (of I) gives
-    // the result.
+    // A pair's lanes hold its reads' rows and at least one pass-through row
+    // below each: the first (row L) holds the value whose sum over a
+    // haplotype's columns gives the result, and the rows below copy it down.
+    // Scaled form: the last lane's last row (the sum row) has emission 1, so
+    // its M is that value one column back and its D (dd = 1) the exact
+    // running sum of the earlier columns: D + M at a separator column is the
+    // sum, with no add per step.  Per-row form: a running sum of I of the last
+    // row (acc_i).
     V acc_i = P::zero();
     // through the virtual end separator of the longer chain, for every
     // pair's last lane
@@ -960,17 +979,21 @@ struct Forward {
         cells(e, up_m, up_i, up_d, dg_m, dg_i, dg_d, M, I, D, pr, t_last);
       }
       (void)t_last;
-      acc_i = P::add(acc_i, I[R - 1]);
+      if constexpr (!kScaled) acc_i = P::add(acc_i, I[R - 1]);
       if (s == nxt) {  // this lane just computed a separator column
+        const V sum = kScaled ? P::add(D[R - 1], M[R - 1]) : acc_i;
 #pragma unroll
         for (int k = 0; k < R; ++k) D[k] = P::zero();
+        if constexpr (kScaled)
+          M[R - 1] = P::zero();  // the sum row's value of the last column
+        else
+          acc_i = P::zero();
         // a pair's sums over haplotype hi (x and y halves), parked in the x
         // read's result slot until the sweep ends
         const uint32_t px = park[lane];
         if (px != kNoStore)
           reinterpret_cast<float2*>(b.out)[px + hi * meta->stride] =
-              make_float2(P::sx(acc_i), P::sy(acc_i));
-        acc_i = P::zero();
+              make_float2(P::sx(sum), P::sy(sum));
         ++hi;
         nxt = (int)meta->sep[hi] + lag;
       }

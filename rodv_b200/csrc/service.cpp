@@ -125,7 +125,7 @@ uint64_t Service::estimate_bytes(const rodv_batch& b, uint64_t pairs) const {
   bytes += 3 * kHapPad + max_h;
   for (uint32_t r = 0; r < b.num_reads; ++r) {
     bytes += (uint64_t)((b.read_lengths[r] + 3) & ~3u) * 4;
-    multi = multi || b.read_lengths[r] >= (uint32_t)kPassRows;
+    multi = multi || b.read_lengths[r] + 2 > (uint32_t)kPassRows;  // class_of, either form
   }
   bytes += (uint64_t)(b.num_haps + b.num_reads) * 16;
   bytes += pairs * (16 + 12 + 8);
