@@ -445,6 +445,45 @@ def test_chain_length_does_not_change_results(engine):
     assert np.array_equal(many[-n:], alone)
 
 
+def test_stacked_read_pairs_match_one_pair_items(engine):
+    """Read pairs stacked down the lanes of one chain item (a region with many
+    uniform-gap reads, packed into multi-pair items of whatever class is
+    cheapest) give bitwise the results the same two reads give as the only
+    pair of a region (one pair per item, the class of the longer read): a
+    read's arithmetic does not depend on its partner, lanes, item or class.
+    Lengths include each class's last (32R - 2 bases) and a multiple of 32."""
+    rng = np.random.default_rng(77)
+    base = np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, 320)]
+    haps = []
+    for k in range(6):
+        h = base[:180 + 16 * k].copy()
+        h[rng.random(len(h)) < 0.02] = ord("T")
+        haps.append(h)
+    lens = [20, 30, 31, 33, 50, 62, 64, 70, 94, 95, 100, 120, 126, 127, 150, 158, 160, 190,
+            222, 224, 230, 254, 40, 45, 55, 60, 75, 80, 85, 90, 105, 110, 115, 135, 140, 170,
+            200, 210, 240, 250]
+    reads, q, ins, gcp = [], [], [], []
+    for L in lens:
+        st = int(rng.integers(0, 320 - L))
+        reads.append(base[st:st + L].copy())
+        q.append(rng.integers(10, 41, L).astype(np.uint8))
+        ins.append(np.full(L, 45, np.uint8))
+        gcp.append(np.full(L, 10, np.uint8))
+    n = len(reads)
+    big_batch = Batch.from_regions([(haps, reads, q, ins, ins, gcp)])
+    big = engine.batch(big_batch)
+    assert np.abs(big - oracle.batch_log10(big_batch)).max() < TOL
+    for i, j in ((0, 1), (4, 21), (13, 14), (18, 19), (21, 39), (2, 3)):
+        pair = [i, j]
+        small = engine.batch(Batch.from_regions([(haps, [reads[k] for k in pair],
+                                                  [q[k] for k in pair], [ins[k] for k in pair],
+                                                  [ins[k] for k in pair],
+                                                  [gcp[k] for k in pair])]))
+        for h in range(len(haps)):
+            assert small[h * 2] == big[h * n + i], (i, j, h)
+            assert small[h * 2 + 1] == big[h * n + j], (i, j, h)
+
+
 def test_chunked_host_path_matches_resident(engine):
     """A batch large enough for the pipelined host-buffer path (region ranges
     packed and uploaded while the previous range computes) gives bitwise the
