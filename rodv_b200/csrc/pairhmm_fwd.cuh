@@ -22,14 +22,18 @@
 //
 // Rows past the end of the read are "pass-through" rows: emission 0, so
 // M = 0, and mi = ii = 1 (I = M_above + I_above), md = 0 (D stays 0).  The
-// value M + I of the read's last row therefore travels unchanged to lane 31's
-// last row, whose running column sum is the result; no lane needs to know
-// which register holds the last row.
+// value M + I of the read's last row therefore travels unchanged down to the
+// last lane's last row, whose column sum is the result; no lane needs to know
+// which register holds the last row.  Chain sweeps (run_chain) stack several
+// read pairs down the lanes, each with its own first lane (row 0's boundary)
+// and last lane; in the scaled form a pair's last row is a sum row whose D
+// keeps that column sum.
 //
 // Emission.  e(i,j) depends on the read base of row i and the haplotype base
 // of column j.  Each lane keeps, in shared memory, a table E[code][k] of its
-// rows' emissions for each of the five haplotype codes, laid out so that the
-// per-step loads are conflict-free 16-byte vector loads.
+// rows' emissions for each of the six haplotype codes (A, C, G, T, N and the
+// separator between a chain's haplotypes), laid out so that the per-step
+// loads are conflict-free 16-byte vector loads.
 //
 // Precision policies.  F32x2 packs two independent pairs into the two halves
 // of the sm_100 f32x2 instructions (fma / add / mul .rn.f32x2), so
@@ -47,12 +51,11 @@
 // pairing); separate per-slot tables, scalar emission multiplies, and the
 // shorter haplotype's running sum frozen when its last column has passed.
 //
-// Uniform-gap form.  When a read's ins/del/gcp quals are constant (GATK data,
-// and every benchmark config), the kernel stores M~ = M/gapm instead of M:
-//   M~ = e*(mm*M~_d + I_d + D_d),  I = (mi*gapm)*M~_u + ii*I_u,
-//   D = (md*gapm)*M~_l + dd*D_l
-// which is 7 arithmetic instructions per cell instead of 8.  The result is
-// gapm*sum(M~) + sum(I).
+// Uniform-gap form.  When a read's ins/del/gcp quals are constant, ins == del
+// and mi*gapm >= 1e-6 (GATK data, and every benchmark config), the kernels run
+// the scaled 5-operation form (load_rows): M~ = M/gapm, I^ = I/c, D^ = D/c
+// with c = mi*gapm folded into the emission table, 5 arithmetic instructions
+// per cell instead of 8.
 //
 // MINB is the launch-bounds occupancy target (blocks per SM); it caps the
 // registers per thread and is chosen per work class by the autotuner.
