@@ -374,6 +374,21 @@ rodv_status rodv_fault_inject_alloc(int32_t kind, int64_t nth);
  * path with no hang and no fault; the device stays usable. */
 rodv_status rodv_fault_inject_wait(int32_t enable);
 void rodv_debug_live_allocations(uint64_t* device, uint64_t* pinned_host);
+/* The chain items the packer makes of one region's reads, on the host only
+ * (no device call; for tests of the placement rules).  Reads 0..num_reads-1
+ * have read_lengths[r] bases and uniform[r] != 0 when their gap priors are
+ * uniform (constant ins/del/gcp, ins == del, as the packer decides from the
+ * qualities); items_per_warp[R - 1] (R = 1..8) is 1, or 2 for the
+ * lane-grouped variant of the uniform class of R rows per lane; stack != 0
+ * lets uniform reads stack (every batch call does).  out receives
+ * [items, leftover read or 0xFFFFFFFF], then per item [class, pairs, then
+ * x read and y read (or 0xFFFFFFFF) of each pair]; *words_written is set
+ * even when out_words is too small (RODV_ERR_INVALID_ARG then).  Multi-pass
+ * reads are not placed in chain items and appear nowhere. */
+rodv_status rodv_debug_chain_plan(const uint32_t* read_lengths, const uint8_t* uniform,
+                                  uint32_t num_reads, const int32_t* items_per_warp,
+                                  int32_t stack, uint32_t* out, uint32_t out_words,
+                                  uint32_t* words_written);
 
 /* Human-readable name of a status code (static storage). */
 const char* rodv_status_string(rodv_status status);

@@ -152,6 +152,9 @@ SIGNATURES = [
     ("rodv_fault_inject_alloc", ctypes.c_int32, [ctypes.c_int32, ctypes.c_int64]),
     ("rodv_debug_live_allocations", None, [_u64p, _u64p]),
     ("rodv_fault_inject_wait", ctypes.c_int32, [ctypes.c_int32]),
+    ("rodv_debug_chain_plan", ctypes.c_int32, [_u32p, _u8p, ctypes.c_uint32,
+                                               ctypes.POINTER(ctypes.c_int32), ctypes.c_int32,
+                                               _u32p, ctypes.c_uint32, _u32p]),
     ("rodv_status_string", ctypes.c_char_p, [ctypes.c_int32]),
     ("rodv_last_error", ctypes.c_char_p, [ctypes.c_void_p]),
 ]

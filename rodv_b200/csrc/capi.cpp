@@ -5,6 +5,7 @@
 #include <new>
 #include <string>
 
+#include "chain_plan.h"
 #include "engine.h"
 #include "service.h"
 
@@ -232,6 +233,42 @@ rodv_status rodv_fault_inject_wait(int32_t enable) {
 
 void rodv_debug_live_allocations(uint64_t* device, uint64_t* pinned_host) {
   rodv::live_allocations(device, pinned_host);
+}
+
+rodv_status rodv_debug_chain_plan(const uint32_t* read_lengths, const uint8_t* uniform,
+                                  uint32_t num_reads, const int32_t* items_per_warp,
+                                  int32_t stack, uint32_t* out, uint32_t out_words,
+                                  uint32_t* words_written) {
+  if (words_written) *words_written = 0;
+  if ((num_reads && (!read_lengths || !uniform)) || !items_per_warp || !words_written ||
+      (out_words && !out))
+    return RODV_ERR_INVALID_ARG;
+  std::vector<uint8_t> cls(num_reads);
+  for (uint32_t r = 0; r < num_reads; ++r) {
+    if (read_lengths[r] == 0 || read_lengths[r] > RODV_MAX_READ_LEN) return RODV_ERR_INVALID_ARG;
+    cls[r] = (uint8_t)rodv::class_of(read_lengths[r], uniform[r] != 0);
+  }
+  int ipw[rodv::kMaxRowsPerLane + 1] = {};
+  for (int R = 1; R <= rodv::kMaxRowsPerLane; ++R) {
+    if (items_per_warp[R - 1] != 1 && items_per_warp[R - 1] != 2) return RODV_ERR_INVALID_ARG;
+    ipw[R] = items_per_warp[R - 1];
+  }
+  rodv::ChainGeom geom[rodv::kMaxRowsPerLane + 1];
+  rodv::chain_geometry(ipw, geom);
+  std::vector<uint32_t> sr;
+  rodv::sort_single_pass(read_lengths, cls.data(), 0, num_reads, sr);
+  rodv::RegionChains rc;
+  rodv::plan_region_chains(read_lengths, cls.data(), geom, stack != 0, sr, rc);
+  std::vector<uint32_t> words{(uint32_t)rc.items.size(), rc.leftover};
+  for (const rodv::ChainPairs& it : rc.items) {
+    words.push_back((uint32_t)it.cls);
+    words.push_back(it.pairs);
+    for (uint32_t j = 0; j < 2 * it.pairs; ++j) words.push_back(rc.reads[it.first + j]);
+  }
+  *words_written = (uint32_t)words.size();
+  if (words.size() > out_words) return RODV_ERR_INVALID_ARG;
+  std::memcpy(out, words.data(), words.size() * 4);
+  return RODV_OK;
 }
 
 const char* rodv_last_error(rodv_engine* engine) {

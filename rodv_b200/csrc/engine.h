@@ -20,14 +20,14 @@ namespace rodv {
 constexpr int kSinglePassClasses = kMaxRowsPerLane * 2;
 constexpr int kNumClasses = kSinglePassClasses + 2;
 
+// The single-pass class of R rows per lane and the given gap form.
+inline int single_pass_class(int R, bool uniform) { return (R - 1) * 2 + (uniform ? 1 : 0); }
 // A single-pass sweep holds a read's rows, then at least one pass-through
 // row (so one running sum gives the result) and, in the uniform-gap (scaled)
 // form, the row whose D sums that pass-through row over each haplotype's
 // columns: a class of R rows per lane holds reads of up to 32R - 1 bases
 // with per-row gaps and 32R - 2 with uniform gaps.  Longer reads are
 // multi-pass.
-// The single-pass class of R rows per lane and the given gap form.
-inline int single_pass_class(int R, bool uniform) { return (R - 1) * 2 + (uniform ? 1 : 0); }
 inline int class_of(uint32_t read_len, bool uniform) {
   const uint32_t rows = read_len + (uniform ? 2u : 1u);
   if (rows <= (uint32_t)kPassRows)
