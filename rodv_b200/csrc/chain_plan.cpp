@@ -13,9 +13,10 @@ namespace {
 // Time per computed cell (lane rows x columns, padding included) of the
 // uniform-gap chain kernels by rows per lane R, relative to R = 8: the
 // autotuner's per-class batches (reads of 32R - 5 bases, one read pair per
-// item) on B200 with each class's fastest variant.  R <= 4 run as two
-// 16-lane items per warp with 2R rows per lane, hence their closeness to
-// R = 8.
+// item) on B200 with each class's fastest variant, measured with a running
+// sum per step (with the sum row they agree within 3%, R = 4 excepted at
+// 1.089).  R <= 4 run as two 16-lane items per warp with 2R rows per lane,
+// hence their closeness to R = 8.
 constexpr double kChainCellCost[kMaxRowsPerLane + 1] = {0.0,   1.53,  1.20,  1.09, 1.024,
                                                         1.093, 1.047, 1.031, 1.0};
 
