@@ -15,6 +15,9 @@
    read row r from M or I at some column and the rest of a path multiplies by
    factors <= 1, so the likelihood is at most sum_j (M + I)[r][j] for every
    row r, per-row gap qualities included.
+3. The chain sweeps' sum row (float32, one rounding per operation): D + M of
+   a last row with emission 1 and dd = 1 at a separator column is bitwise the
+   running sum of the pass-through value over the haplotype's columns.
 
 The priors here are plain float64 formulas (ph2pr[q] = 10^(-q/10), mm = 1 -
 ph2pr[ins] - ph2pr[del]); both forms use the same ones, so the comparison is
@@ -117,3 +120,115 @@ def test_row_sums_bound_the_likelihood(uniform):
         for r in range(1, L + 1):
             bound = M[r, 1:].sum() + I[r, 1:].sum()
             assert lik <= bound * (1 + 1e-12), (r, lik, bound)
+
+
+# ---- float32 chain sweep: the sum row against a running sum -----------------
+#
+# The chain kernels sweep one read (per f32x2 half) across several
+# haplotypes laid end to end with a separator column between them (emission
+# 0 in every row; each row's D cleared after it).  Below the read's rows sit
+# pass-through rows (emission 0; ii = mi on the first, 1 below), so the last
+# row carries the value whose column sum per haplotype is the result.  The
+# kernels once added that value into a running sum every step; now the last
+# row is a sum row with emission 1 for every code, and D takes each row's ii,
+# so the sum row's M is the value one column back and its D = D + M the sum
+# of the earlier columns: D + M at the separator column is the haplotype's
+# sum.  Emulated in float32 with one rounding per operation (as the kernels'
+# .rn PTX), the two must give bitwise the same sums.
+
+def _f32(x):
+    return np.float32(x)
+
+
+def _fma(a, b, c):
+    return np.float32(np.float64(a) * np.float64(b) + np.float64(c))
+
+
+def _mul(a, b):
+    return np.float32(np.float64(a) * np.float64(b))
+
+
+def _add(a, b):
+    return _fma(1.0, a, b)
+
+
+def chain_sweep_f32(read, haps, p, init, rows, sum_row):
+    """Per-haplotype parked sums of a float32 scaled chain sweep."""
+    L = len(read)
+    mi, gapm, mm, ii, dd = (float(p[k][0]) for k in ("mi", "gapm", "mm", "ii", "dd"))
+    c = mi * gapm
+    mmc = _f32(mm / c)
+    iis = [_f32(ii) if r < L else (_f32(mi) if r == L else _f32(1.0)) for r in range(rows)]
+    ddU = _f32(dd)
+    # emission rows of every column of the chain (None: separator column)
+    cols = []
+    for k, hap in enumerate(haps):
+        E = (emissions(read, hap, p) * c).astype(np.float32)
+        for j in range(len(hap)):
+            cols.append(E[:, j])
+        cols.append(None)
+    M = [_f32(0)] * rows; I = [_f32(0)] * rows; D = [_f32(0)] * rows
+    acc = _f32(0)
+    parked = []
+    for col in cols:
+        e = [_f32(0)] * rows
+        if col is not None:
+            e[:L] = [_f32(v) for v in col]
+        if sum_row:
+            e[rows - 1] = _f32(1.0)
+        oM, oI, oD = M, I, D
+        M = [None] * rows; I = [None] * rows; D = [None] * rows
+        for r in range(rows):
+            if r == 0:
+                t = _f32(init)              # row 0's boundary, D^ = init
+                I[0] = _f32(0)
+            else:
+                t = _fma(mmc, oM[r - 1], _add(oI[r - 1], oD[r - 1]))
+                I[r] = _fma(iis[r], I[r - 1], M[r - 1])
+            M[r] = _mul(t, e[r])
+            D[r] = _fma(iis[r] if sum_row else ddU, oD[r], oM[r])
+        if not sum_row:
+            acc = _add(acc, I[rows - 1])
+        if col is None:                     # a separator column
+            if sum_row:
+                parked.append(_add(D[rows - 1], M[rows - 1]))
+                M[rows - 1] = _f32(0)
+            else:
+                parked.append(acc)
+                acc = _f32(0)
+            D = [_f32(0)] * rows
+    return parked
+
+
+@pytest.mark.parametrize("L,rows", [(12, 16), (14, 16), (15, 18), (30, 40)])
+def test_sum_row_gives_the_running_sum_bitwise(L, rows):
+    rng = np.random.default_rng(L * 7 + rows)
+    haps = [rng.integers(0, 4, int(rng.integers(L // 2, 2 * L))) for _ in range(3)]
+    read = haps[0][:L].copy() if len(haps[0]) >= L else rng.integers(0, 4, L)
+    read[rng.random(L) < 0.1] = 0
+    p = priors(rng.integers(10, 41, L), np.full(L, 45), np.full(L, 45), np.full(L, 10))
+    init = 2.0 ** 120 / max(len(h) for h in haps)
+    old = chain_sweep_f32(read, haps, p, init, rows, sum_row=False)
+    new = chain_sweep_f32(read, haps, p, init, rows, sum_row=True)
+    assert len(old) == len(new) == len(haps)
+    for a, b in zip(old, new):
+        assert a.tobytes() == b.tobytes(), (a, b)
+    # and both are the likelihood (times mi) of each haplotype's own DP, with
+    # row 0's D = init in every column, column 0 included (the reference's
+    # initialisation, which the sweeps apply as row 0's M term at every step;
+    # reference_dp above leaves column 0 at zero for the algebra tests)
+    for h, got in zip(haps, new):
+        H = len(h)
+        E = emissions(read, h, p)
+        M = np.zeros((L + 1, H + 1)); I = np.zeros_like(M); D = np.zeros_like(M)
+        D[0, :] = init
+        for i in range(1, L + 1):
+            r = i - 1
+            M[i, 1:] = E[r] * (p["mm"][r] * M[i - 1, :-1] +
+                               p["gapm"][r] * (I[i - 1, :-1] + D[i - 1, :-1]))
+            I[i, 1:] = p["mi"][r] * M[i - 1, 1:] + p["ii"][r] * I[i - 1, 1:]
+            for j in range(1, H + 1):
+                D[i, j] = p["md"][r] * M[i, j - 1] + p["dd"][r] * D[i, j - 1]
+        ref = (M[L, 1:].sum() + I[L, 1:].sum()) * float(p["mi"][0])
+        assert ref > 0
+        assert abs(float(got) - ref) <= 2e-4 * ref, (float(got), ref)
